@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Distance-index build benchmark (one JSON line on rank 0).
+
+Workload: the plain index build at chromosome scale -- a synthetic sequence
+graph of 5e7 backbone bases (SNP 1/1000, indel 1/5000 with geometric length
+mean 4 capped at 50, 0.1 % of bubbles structural with length 100..2000, seed
+42), adjacency in range CRS with uint32 columns, index = A^400 * (A+I)^200
+(distance window [400, 600]).  A step is one complete index build.
+
+  value    seconds per build with A already resident in HBM (device time over
+           the timed steps, CUDA events on the library's stream, max over ranks)
+  e2e      the same through the C ABI with host buffers: every step copies A
+           from pinned host memory, builds, and copies the index back
+  roofline the range-SpGEMM kernel (symbolic + numeric passes): algorithmic
+           bytes (read A and B once, write C once) / its event-timed duration
+  cpu_baseline the CPU restatement of the reference's bitvector SpGEMM path
+           (OpenMP, all host threads) on a prefix of the same graph, scaled
+
+--impl reference times that CPU restatement alone (the reference's own
+Kokkos/OpenMP build cannot be compiled: its submodules are absent).
+With N GPUs each rank builds its own graph (seed 42 + rank): the index is
+block-diagonal over independent components, so ranks share no data.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n-backbone", type=int, default=50_000_000)
+    p.add_argument("--dmin", type=int, default=400)
+    p.add_argument("--dmax", type=int, default=600)
+    p.add_argument("--seed", type=int, default=42)
+    p.add_argument("--cpu-target-s", type=float, default=12.0,
+                   help="wall seconds the CPU baseline sample should take")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, devices):
+        self.devices = devices
+        self.proc = None
+        self.tmp = None
+
+    def __enter__(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ",".join(map(str, self.devices)), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.tmp is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self.tmp.flush()
+        rows = []
+        with open(self.tmp.name) as f:
+            for ln in f:
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples"]}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+def graph(n_backbone, seed):
+    from diverg_b200 import gen
+    spec = gen.chromosome_graph_spec(n_backbone, seed=seed)
+    return gen.graph_adjacency(spec)
+
+
+def cpu_build_seconds(n_backbone, seed, dmin, dmax):
+    """One index build by the CPU restatement (bitvector SpGEMM, OpenMP)."""
+    from oracle import pyoracle as orc
+    a, _ = graph(n_backbone, seed)
+    oa = orc.OMat(a.numRows(), a.numCols(), a.rowmap, a.entries, a.nnz())
+    t = time.perf_counter()
+    orc.dindex(oa, dmin, dmax, algo="hbv")
+    return time.perf_counter() - t, a.numRows()
+
+
+def cpu_sample_plan(args, n_full_loci):
+    """Prefix size whose CPU build takes about args.cpu_target_s seconds."""
+    t1, loci1 = cpu_build_seconds(1_000_000, args.seed, args.dmin, args.dmax)
+    per_locus = t1 / loci1
+    n_sample = int(min(args.n_backbone, max(1_000_000, args.cpu_target_s / per_locus)))
+    return n_sample
+
+
+def cpu_baseline(args, n_full_loci):
+    from oracle import pyoracle as orc
+    n_sample = cpu_sample_plan(args, n_full_loci)
+    t, loci = cpu_build_seconds(n_sample, args.seed, args.dmin, args.dmax)
+    scaled = t * n_full_loci / loci
+    return {"value": scaled, "unit": "s", "cores": orc.threads(), "kind": "port",
+            "sample": f"index build [{args.dmin},{args.dmax}] of the first {n_sample:.3g} backbone bases "
+                      f"({loci} loci) of the same graph generator, {t:.2f} s, scaled x{n_full_loci / loci:.1f} "
+                      f"to {n_full_loci} loci; CPU restatement of the reference's bitvector SpGEMM path "
+                      f"(OpenMP, {orc.threads()} threads), not the reference binary"}
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the restated reference path on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import pyoracle as orc
+    from diverg_b200 import gen
+    spec = gen.chromosome_graph_spec(args.n_backbone, seed=args.seed)
+    _, st = gen.graph_adjacency(spec)
+    n_full = st["n_loci"]
+    n_sample = cpu_sample_plan(args, n_full)
+    times = []
+    loci = None
+    for i in range(args.warmup + args.steps):
+        t, loci = cpu_build_seconds(n_sample, args.seed, args.dmin, args.dmax)
+        if i >= args.warmup:
+            times.append(t * n_full / loci)
+    value = sum(times) / len(times)
+    line = {
+        "impl": "reference", "metric": "index-build s", "value": value, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": config_dict(args, n_full),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": orc.threads(), "kind": "port",
+                         "sample": f"each step: index build of the first {n_sample:.3g} backbone bases ({loci} "
+                                   f"loci), scaled to {n_full} loci; CPU restatement (OpenMP) of the reference's "
+                                   f"bitvector SpGEMM path: the reference's Kokkos build cannot be compiled here"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args, n_loci):
+    return {"workload": "plain index build, synthetic chromosome-scale sequence graph",
+            "n_backbone": args.n_backbone, "n_loci": n_loci, "window": [args.dmin, args.dmax],
+            "bubbles": "SNP 1/1000, indel 1/5000 (geometric mean 4, cap 50), 0.1% structural (100..2000)",
+            "seed": args.seed, "index_types": "uint32 columns, uint64 rowmap",
+            "l2": "inputs larger than L2 (A and every intermediate exceed 126 MB)",
+            "parallelism": f"{args.gpus} independent graph(s), one per GPU"}
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from diverg_b200.runtime import Context
+
+    a, gstats = graph(args.n_backbone, args.seed + rank)
+    n_loci = a.numRows()
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    d_a = ctx.upload(a)
+
+    idx = None
+    for _ in range(args.warmup):
+        idx = ctx.distance_index(d_a, args.dmin, args.dmax)
+        if _ < args.warmup - 1:
+            idx.free()
+    idx_rows, idx_entries, idx_nnz = idx.nrows, idx.nentries, idx.nnz
+    idx.free()
+
+    # ---- timed: device-resident input -------------------------------------
+    ctx.set_option("timing", 1)
+    ctx.reset_stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler([local] if world == 1 else list(range(world))) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            idx = ctx.distance_index(d_a, args.dmin, args.dmax)
+            idx.free()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms_total = max_over_ranks(ev0.elapsed_time(ev1))
+    st = ctx.stats()
+    ctx.set_option("timing", 0)
+    sec_per_build = ms_total / 1e3 / args.steps
+
+    # ---- e2e: host buffers through the C ABI ---------------------------------
+    e2e = None
+    if not args.no_e2e:
+        h_rowmap = torch.from_numpy(a.rowmap.astype(np.uint64).view(np.int64)).pin_memory()
+        h_entries = torch.from_numpy(a.entries.view(np.int32)).pin_memory()
+        o_rowmap = torch.empty(idx_rows + 1, dtype=torch.int64).pin_memory()
+        o_entries = torch.empty(max(1, idx_entries), dtype=torch.int32).pin_memory()
+        h2d = h_rowmap.numel() * 8 + h_entries.numel() * 4
+        d2h = (idx_rows + 1) * 8 + idx_entries * 4
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            da2 = ctx.upload_arrays(n_loci, n_loci, h_rowmap.data_ptr(), h_entries.data_ptr(), a.nnz())
+            ix = ctx.distance_index(da2, args.dmin, args.dmax)
+            ix.download_to(o_rowmap.data_ptr(), o_entries.data_ptr())
+            ix.free()
+            da2.free()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_s = max_over_ranks(e0.elapsed_time(e1)) / 1e3 / args.steps
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- roofline of the range-SpGEMM kernel ------------------------------
+    peak, peak_kind = peaks()
+    spgemm_ns = st["spgemm_symbolic_ns"] + st["spgemm_numeric_ns"]
+    spgemm_calls = max(1, st["spgemm_calls"])
+    per_product_bytes = st["spgemm_alg_bytes"] / spgemm_calls
+    per_product_s = spgemm_ns / 1e9 / spgemm_calls
+    achieved = per_product_bytes / per_product_s / 1e9 if per_product_s > 0 else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "peak_kind": peak_kind,
+                "kernel": "k_spgemm_rows (symbolic + numeric passes of one range SpGEMM)",
+                "alg_bytes_per_product": per_product_bytes, "products_per_build": st["spgemm_calls"] / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, n_loci)
+
+    if rank == 0:
+        steps = args.steps
+        line = {
+            "metric": "index-build s", "value": sec_per_build, "unit": "s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": sec_per_build * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": config_dict(args, n_loci),
+            "e2e": e2e,
+            "gpu_launches": st["kernel_launches"],
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "build": {"index_rows": idx_rows, "index_ranges": idx_entries // 2, "index_nnz": idx_nnz,
+                      "graph": gstats, "spgemm_per_build": st["spgemm_calls"] / steps,
+                      "alg_gb_per_build": st["alg_bytes"] / steps / 1e9,
+                      "build_gbs": st["alg_bytes"] / steps / 1e9 / sec_per_build,
+                      "kernel_ms_per_build": {
+                          "spgemm_symbolic": st["spgemm_symbolic_ns"] / 1e6 / steps,
+                          "spgemm_numeric": st["spgemm_numeric_ns"] / 1e6 / steps,
+                          "scan": st["scan_ns"] / 1e6 / steps, "spadd": st["spadd_ns"] / 1e6 / steps},
+                      "host_syncs_per_build": st["host_syncs"] / steps,
+                      "range_ops_per_build": st["range_ops"] / steps},
+        }
+        print(json.dumps(line), flush=True)
+
+    d_a.free()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

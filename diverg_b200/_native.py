@@ -1,0 +1,140 @@
+"""ctypes bindings of libdvg.so (include/dvg.h) and libdvg_gen.so (include/dvg_gen.h).
+
+The CUDA library is the only compute path: when it is missing or no sm_100
+device is present, every call raises; there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdvg.so")
+GEN_PATH = os.path.join(_HERE, "libdvg_gen.so")
+
+# dvg_status
+OK, INVALID_ARG, OOM, DEVICE, TIMEOUT, NOT_INITIALIZED, OVERFLOW = range(7)
+
+
+class DvgError(RuntimeError):
+    """A non-OK dvg_status; `status` holds the code."""
+
+    def __init__(self, status, msg):
+        super().__init__(msg)
+        self.status = status
+
+
+class DvgStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "kernel_launches", "spgemm_calls", "spadd_calls", "host_syncs", "alg_bytes",
+        "spgemm_alg_bytes", "range_ops", "h2d_bytes", "d2h_bytes", "spgemm_symbolic_ns", "spgemm_numeric_ns",
+        "scan_ns", "spadd_ns")]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+class HostMatrix(ctypes.Structure):
+    _fields_ = [("nrows", ctypes.c_uint32), ("ncols", ctypes.c_uint32), ("nentries", ctypes.c_uint64),
+                ("nnz", ctypes.c_uint64), ("rowmap", ctypes.POINTER(ctypes.c_uint64)),
+                ("entries", ctypes.POINTER(ctypes.c_uint32))]
+
+
+class GraphParams(ctypes.Structure):
+    _fields_ = [("n_backbone", ctypes.c_uint64), ("snp_rate", ctypes.c_double), ("indel_rate", ctypes.c_double),
+                ("ins_frac", ctypes.c_double), ("indel_lmin", ctypes.c_uint32), ("indel_lmax", ctypes.c_uint32),
+                ("indel_geometric_mean", ctypes.c_double), ("sv_frac", ctypes.c_double),
+                ("sv_lmin", ctypes.c_uint32), ("sv_lmax", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+class GraphStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "n_loci", "n_snp", "n_ins", "n_del", "n_sv", "n_alt_loci")]
+
+
+# Every entry point of include/dvg.h with its argument types.
+_P, _U32, _U64, _I64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int64
+_PP = ctypes.POINTER(ctypes.c_void_p)
+DVG_SIGNATURES = {
+    "dvg_init": [ctypes.c_int, _PP],
+    "dvg_shutdown": [_P],
+    "dvg_set_stream": [_P, _P],
+    "dvg_synchronize": [_P],
+    "dvg_set_option": [_P, ctypes.c_char_p, _I64],
+    "dvg_get_stats": [_P, ctypes.POINTER(DvgStats)],
+    "dvg_stats_reset": [_P],
+    "dvg_last_error": [],
+    "dvg_status_string": [ctypes.c_int],
+    "dvg_matrix_upload": [_P, _U32, _U32, _P, _P, _U64, _PP],
+    "dvg_matrix_upload_u32": [_P, _U32, _U32, _P, _P, _U64, _PP],
+    "dvg_matrix_wrap_device": [_P, _U32, _U32, _P, _P, _U64, _U64, _PP],
+    "dvg_matrix_info": [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U64), ctypes.POINTER(_U64)],
+    "dvg_matrix_device_arrays": [_P, _PP, _PP],
+    "dvg_matrix_download": [_P, _P, _P, _P],
+    "dvg_matrix_download_u32": [_P, _P, _P, _P],
+    "dvg_matrix_free": [_P, _P],
+    "dvg_range_identity": [_P, _U32, _PP],
+    "dvg_range_spadd": [_P, _P, _P, _PP],
+    "dvg_range_spgemm": [_P, _P, _P, _PP],
+    "dvg_range_power": [_P, _P, ctypes.c_uint, _PP],
+    "dvg_create_distance_index": [_P, _P, ctypes.c_uint, ctypes.c_uint, _PP],
+    "dvg_query_batch": [_P, _P, _P, _U64, _P],
+    "dvg_query_batch_host": [_P, _P, _P, _U64, _P],
+}
+
+GEN_SIGNATURES = {
+    "dvg_gen_graph_adjacency": [ctypes.POINTER(GraphParams), ctypes.POINTER(HostMatrix), ctypes.POINTER(GraphStats)],
+    "dvg_gen_graph_edges": [ctypes.POINTER(GraphParams), ctypes.POINTER(_U64), ctypes.POINTER(_U64),
+                            ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32))],
+    "dvg_gen_banded": [_U32, _U32, ctypes.c_double, ctypes.c_double, _U64, ctypes.POINTER(HostMatrix)],
+    "dvg_gen_random": [_U32, _U64, _U64, ctypes.POINTER(HostMatrix)],
+    "dvg_gen_pairs": [ctypes.POINTER(HostMatrix), _U64, ctypes.c_double, _U32, _U32, _U64, _P],
+    "dvg_gen_free": [ctypes.POINTER(HostMatrix)],
+    "dvg_gen_free_ptr": [_P],
+}
+
+_lib = None
+_gen = None
+
+
+def lib():
+    """The CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                               "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in DVG_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.dvg_last_error.restype = ctypes.c_char_p
+        L.dvg_status_string.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def gen_lib():
+    global _gen
+    if _gen is None:
+        if not os.path.exists(GEN_PATH):
+            raise RuntimeError(f"{GEN_PATH} is missing: build it with __graft_entry__.build()")
+        L = ctypes.CDLL(GEN_PATH)
+        for name, args in GEN_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = None if name.startswith("dvg_gen_free") else ctypes.c_int
+        _gen = L
+    return _gen
+
+
+def check(status):
+    if status != OK:
+        L = lib()
+        msg = L.dvg_last_error().decode(errors="replace")
+        raise DvgError(status, f"{L.dvg_status_string(status).decode()}: {msg}")
+
+
+def ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)

@@ -1,0 +1,700 @@
+// dvg_api.cu -- the C ABI of include/dvg.h and the host orchestration of the
+// range operations: products, sums, powers and the distance index.  Every
+// entry point converts internal failures into a dvg_status.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "dvg_internal.h"
+
+namespace {
+thread_local std::string g_last_error;
+
+dvg_status fail(dvg_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+template <class F>
+dvg_status guarded(F&& f) {
+  try {
+    f();
+    return DVG_OK;
+  } catch (const dvg::Error& e) {
+    return fail(e.status, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(DVG_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(DVG_ERR_DEVICE, e.what());
+  }
+}
+
+void require(bool ok, const char* msg) {
+  if (!ok) throw dvg::Error(DVG_ERR_INVALID_ARG, msg);
+}
+
+struct Lock {
+  dvg_context* ctx;
+  explicit Lock(dvg_context* c) : ctx(c) {
+    require(c != nullptr, "null context");
+    ctx->mu.lock();
+    DVG_CUDA(cudaSetDevice(ctx->device));
+  }
+  ~Lock() { ctx->mu.unlock(); }
+};
+}  // namespace
+
+namespace dvg {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  dvg_status s = (e == cudaErrorMemoryAllocation) ? DVG_ERR_OOM : DVG_ERR_DEVICE;
+  throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void* dalloc(dvg_context* ctx, size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? DVG_ERR_OOM : DVG_ERR_DEVICE,
+                std::string("device allocation of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+  }
+  return p;
+}
+
+void dfree(dvg_context* ctx, void* p) {
+  if (p) DVG_CUDA(cudaFreeAsync(p, ctx->stream));
+}
+
+static size_t entries_alloc_bytes(uint64_t nentries) {
+  // padded to 16 bytes so vector loads of the last range stay inside
+  return size_t((nentries * 4 + 15) / 16 * 16 + 16);
+}
+
+dvg_matrix* new_matrix(dvg_context* ctx, uint32_t nrows, uint32_t ncols, uint64_t nentries) {
+  auto* m = new dvg_matrix();
+  m->nrows = nrows;
+  m->ncols = ncols;
+  m->nentries = nentries;
+  m->device = ctx->device;
+  try {
+    m->rowmap = static_cast<uint64_t*>(dalloc(ctx, (size_t(nrows) + 1) * sizeof(uint64_t)));
+    m->entries = static_cast<uint32_t*>(dalloc(ctx, entries_alloc_bytes(nentries)));
+  } catch (...) {
+    free_matrix(ctx, m);
+    throw;
+  }
+  return m;
+}
+
+void free_matrix(dvg_context* ctx, dvg_matrix* m) {
+  if (!m) return;
+  if (m->owned) {
+    dfree(ctx, m->rowmap);
+    dfree(ctx, m->entries);
+  }
+  delete m;
+}
+
+static cudaEvent_t take_event(dvg_context* ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  DVG_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+cudaEvent_t span_begin(dvg_context* ctx) {
+  if (!ctx->opt_timing) return nullptr;
+  cudaEvent_t e = take_event(ctx);
+  DVG_CUDA(cudaEventRecord(e, ctx->stream));
+  return e;
+}
+
+void span_end(dvg_context* ctx, cudaEvent_t begin, TimedKind kind) {
+  if (!begin) return;
+  cudaEvent_t e = take_event(ctx);
+  DVG_CUDA(cudaEventRecord(e, ctx->stream));
+  ctx->timed.push_back({begin, e, int(kind)});
+}
+
+// After a stream synchronisation every recorded span has completed.
+static void resolve_spans(dvg_context* ctx) {
+  for (auto& t : ctx->timed) {
+    float ms = 0.f;
+    DVG_CUDA(cudaEventElapsedTime(&ms, t.begin, t.end));
+    uint64_t ns = uint64_t(double(ms) * 1e6);
+    switch (t.kind) {
+      case kSymbolic: ctx->stats.spgemm_symbolic_ns += ns; break;
+      case kNumeric: ctx->stats.spgemm_numeric_ns += ns; break;
+      case kScan: ctx->stats.scan_ns += ns; break;
+      default: ctx->stats.spadd_ns += ns; break;
+    }
+    ctx->event_pool.push_back(t.begin);
+    ctx->event_pool.push_back(t.end);
+  }
+  ctx->timed.clear();
+}
+
+void reset_control(dvg_context* ctx) {
+  DVG_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, sizeof(DeviceControl), ctx->stream));
+}
+
+DeviceControl read_control(dvg_context* ctx) {
+  DVG_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, ctx->stream));
+  DVG_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->stats.host_syncs++;
+  resolve_spans(ctx);
+  DeviceControl c = *ctx->h_ctl;
+  if (c.status) throw Error(DVG_ERR_DEVICE, "internal consistency check failed on the device (code " +
+                                                std::to_string(c.status) + ")");
+  return c;
+}
+
+// Reads rowmap[n] of a freshly scanned rowmap together with the control block.
+static DeviceControl read_total(dvg_context* ctx, const uint64_t* rowmap_last, uint64_t* total) {
+  uint64_t* h_total = reinterpret_cast<uint64_t*>(ctx->h_ctl + 1);
+  DVG_CUDA(cudaMemcpyAsync(h_total, rowmap_last, sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
+  DeviceControl c = read_control(ctx);
+  *total = *h_total;
+  return c;
+}
+
+dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b) {
+  if (!a_identity) require(a->ncols == b->nrows, "range_spgemm: a.numCols() != b.numRows()");
+  const uint32_t n = a_identity ? b->nrows : a->nrows;
+  dvg_matrix* c = new_matrix(ctx, n, b->ncols, 0);
+  try {
+    DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
+    reset_control(ctx);
+    SpgemmPlan plan = plan_spgemm(ctx, a, a_identity, b);
+    cudaEvent_t t0 = span_begin(ctx);
+    launch_spgemm(ctx, plan, a, a_identity, b, c->rowmap, nullptr, false);
+    span_end(ctx, t0, kSymbolic);
+    t0 = span_begin(ctx);
+    launch_rowmap_scan(ctx, c->rowmap, n);
+    span_end(ctx, t0, kScan);
+    uint64_t total = 0;
+    DeviceControl ctl = read_total(ctx, c->rowmap + n, &total);
+    if (total > 0) {
+      dfree(ctx, c->entries);
+      c->entries = nullptr;
+      c->entries = static_cast<uint32_t*>(dalloc(ctx, entries_alloc_bytes(total)));
+      c->nentries = total;
+      t0 = span_begin(ctx);
+      launch_spgemm(ctx, plan, a, a_identity, b, c->rowmap, c->entries, true);
+      span_end(ctx, t0, kNumeric);
+    }
+    c->nnz = ctl.nnz;
+    ctx->stats.spgemm_calls++;
+    uint64_t bytes = (a_identity ? 0 : matrix_bytes(a)) + matrix_bytes(b) + matrix_bytes(c);
+    ctx->stats.alg_bytes += bytes;
+    ctx->stats.spgemm_alg_bytes += bytes;
+    ctx->stats.range_ops += ctl.range_ops;
+  } catch (...) {
+    free_matrix(ctx, c);
+    throw;
+  }
+  return c;
+}
+
+dvg_matrix* range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity) {
+  if (!b_identity) {
+    require(a->nrows == b->nrows, "range_spadd: row counts differ");
+    require(a->ncols == b->ncols, "range_spadd: column counts differ");
+  } else {
+    require(a->nrows <= a->ncols, "range_spadd: identity does not fit the matrix");
+  }
+  const uint32_t n = a->nrows;
+  dvg_matrix* c = new_matrix(ctx, n, a->ncols, 0);
+  try {
+    DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
+    reset_control(ctx);
+    cudaEvent_t t0 = span_begin(ctx);
+    launch_spadd(ctx, a, b, b_identity, c->rowmap, nullptr, false);
+    span_end(ctx, t0, kSpadd);
+    t0 = span_begin(ctx);
+    launch_rowmap_scan(ctx, c->rowmap, n);
+    span_end(ctx, t0, kScan);
+    uint64_t total = 0;
+    DeviceControl ctl = read_total(ctx, c->rowmap + n, &total);
+    if (total > 0) {
+      dfree(ctx, c->entries);
+      c->entries = nullptr;
+      c->entries = static_cast<uint32_t*>(dalloc(ctx, entries_alloc_bytes(total)));
+      c->nentries = total;
+      t0 = span_begin(ctx);
+      launch_spadd(ctx, a, b, b_identity, c->rowmap, c->entries, true);
+      span_end(ctx, t0, kSpadd);
+    }
+    c->nnz = ctl.nnz;
+    ctx->stats.spadd_calls++;
+    ctx->stats.alg_bytes += matrix_bytes(a) + (b_identity ? 0 : matrix_bytes(b)) + matrix_bytes(c);
+  } catch (...) {
+    free_matrix(ctx, c);
+    throw;
+  }
+  return c;
+}
+
+dvg_matrix* identity(dvg_context* ctx, uint32_t n) {
+  dvg_matrix* m = new_matrix(ctx, n, n, 2ull * n);
+  try {
+    launch_identity(ctx, m);
+  } catch (...) {
+    free_matrix(ctx, m);
+    throw;
+  }
+  m->nnz = n;
+  return m;
+}
+
+// range_power_inplace, range_sparse.hpp:2370-2431: C = I; for each bit of k
+// from the lowest, C <- C*A if it is set, then A <- A*A while bits remain.
+// The first C*A has C = I and runs with an implicit identity operand.
+dvg_matrix* range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k) {
+  require(a->nrows == a->ncols, "range_power: matrix is not square");
+  if (k == 0) return identity(ctx, a->ncols);
+  dvg_matrix* c = nullptr;
+  const dvg_matrix* p = a;  // current power of a (a itself is not owned)
+  try {
+    while (true) {
+      if (k & 1) {
+        dvg_matrix* nc = c ? range_spgemm(ctx, c, false, p) : range_spgemm(ctx, nullptr, true, p);
+        free_matrix(ctx, c);
+        c = nc;
+      }
+      k >>= 1;
+      if (k == 0) break;
+      dvg_matrix* np = range_spgemm(ctx, p, false, p);
+      if (p != a) free_matrix(ctx, const_cast<dvg_matrix*>(p));
+      p = np;
+    }
+  } catch (...) {
+    free_matrix(ctx, c);
+    if (p != a) free_matrix(ctx, const_cast<dvg_matrix*>(p));
+    throw;
+  }
+  if (p != a) free_matrix(ctx, const_cast<dvg_matrix*>(p));
+  return c;
+}
+
+// util::create_distance_index, dindex.hpp:46-189.
+dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup) {
+  require(dlo <= dup && dup != 0, "create_distance_index: requires dmin <= dmax and dmax != 0");
+  require(a->nrows == a->ncols, "create_distance_index: adjacency matrix is not square");
+  dvg_matrix* rai = range_spadd(ctx, a, nullptr, true);  // I + A (fused identity)
+  dvg_matrix* rad = nullptr;
+  dvg_matrix* raid = nullptr;
+  dvg_matrix* d = nullptr;
+  try {
+    if (dlo != 0) rad = range_power(ctx, a, dlo);
+    raid = range_power(ctx, rai, dup - dlo);
+    free_matrix(ctx, rai);
+    rai = nullptr;
+    if (dlo != 0) {
+      d = range_spgemm(ctx, rad, false, raid);
+      free_matrix(ctx, rad);
+      free_matrix(ctx, raid);
+    } else {
+      d = raid;
+    }
+  } catch (...) {
+    free_matrix(ctx, rai);
+    free_matrix(ctx, rad);
+    free_matrix(ctx, raid);
+    throw;
+  }
+  return d;
+}
+
+}  // namespace dvg
+
+using namespace dvg;
+
+extern "C" {
+
+const char* dvg_last_error(void) { return g_last_error.c_str(); }
+
+const char* dvg_status_string(dvg_status s) {
+  switch (s) {
+    case DVG_OK: return "ok";
+    case DVG_ERR_INVALID_ARG: return "invalid argument";
+    case DVG_ERR_OOM: return "out of memory";
+    case DVG_ERR_DEVICE: return "device error";
+    case DVG_ERR_TIMEOUT: return "device wait timed out";
+    case DVG_ERR_NOT_INITIALIZED: return "not initialized";
+    case DVG_ERR_OVERFLOW: return "overflow";
+  }
+  return "unknown";
+}
+
+dvg_status dvg_init(int device, dvg_context** out) {
+  if (!out) return fail(DVG_ERR_INVALID_ARG, "null output pointer");
+  *out = nullptr;
+  dvg_context* ctx = new dvg_context();
+  dvg_status s = guarded([&] {
+    int count = 0;
+    DVG_CUDA(cudaGetDeviceCount(&count));
+    require(device >= 0 && device < count, "no such CUDA device");
+    cudaDeviceProp prop{};
+    DVG_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+      throw Error(DVG_ERR_DEVICE, std::string("libdvg is built for sm_100a (B200); device is ") + prop.name);
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    DVG_CUDA(cudaSetDevice(device));
+    DVG_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+    ctx->stream = ctx->own_stream;
+    cudaMemPool_t pool;
+    DVG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = ~0ull;
+    DVG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    DVG_CUDA(cudaMalloc(&ctx->d_ctl, sizeof(DeviceControl)));
+    DVG_CUDA(cudaMemset(ctx->d_ctl, 0, sizeof(DeviceControl)));
+    // control block mirror plus one word for size read-backs
+    DVG_CUDA(cudaMallocHost(&ctx->h_ctl, 2 * sizeof(DeviceControl)));
+  });
+  if (s != DVG_OK) {
+    if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+    if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return s;
+  }
+  *out = ctx;
+  return DVG_OK;
+}
+
+dvg_status dvg_shutdown(dvg_context* ctx) {
+  if (!ctx) return fail(DVG_ERR_INVALID_ARG, "null context");
+  dvg_status s = guarded([&] {
+    Lock lk(ctx);
+    if (ctx->d_tile_sums) dfree(ctx, ctx->d_tile_sums);
+    if (ctx->d_pairs) dfree(ctx, ctx->d_pairs);
+    if (ctx->d_answers) dfree(ctx, ctx->d_answers);
+    DVG_CUDA(cudaStreamSynchronize(ctx->stream));
+    resolve_spans(ctx);
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    ctx->event_pool.clear();
+    DVG_CUDA(cudaFree(ctx->d_ctl));
+    DVG_CUDA(cudaFreeHost(ctx->h_ctl));
+    if (ctx->own_stream) DVG_CUDA(cudaStreamDestroy(ctx->own_stream));
+  });
+  delete ctx;
+  return s;
+}
+
+dvg_status dvg_set_stream(dvg_context* ctx, void* stream) {
+  return guarded([&] {
+    Lock lk(ctx);
+    DVG_CUDA(cudaStreamSynchronize(ctx->stream));
+    resolve_spans(ctx);
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  });
+}
+
+dvg_status dvg_synchronize(dvg_context* ctx) {
+  return guarded([&] {
+    Lock lk(ctx);
+    read_control(ctx);
+  });
+}
+
+dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(key != nullptr, "null option key");
+    if (!std::strcmp(key, "group_lanes")) {
+      require(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
+              "group_lanes must be 0, 4, 8, 16 or 32");
+      ctx->opt_group_lanes = value;
+    } else if (!std::strcmp(key, "window_words")) {
+      require(value >= 0 && value <= 4096, "window_words must be in [0, 4096]");
+      ctx->opt_window_words = value;
+    } else if (!std::strcmp(key, "timing")) {
+      DVG_CUDA(cudaStreamSynchronize(ctx->stream));
+      resolve_spans(ctx);
+      ctx->opt_timing = value != 0;
+    } else {
+      require(false, "unknown option");
+    }
+  });
+}
+
+dvg_status dvg_get_stats(const dvg_context* ctx, dvg_stats* out) {
+  if (!ctx || !out) return fail(DVG_ERR_INVALID_ARG, "null argument");
+  *out = ctx->stats;
+  return DVG_OK;
+}
+
+dvg_status dvg_stats_reset(dvg_context* ctx) {
+  if (!ctx) return fail(DVG_ERR_INVALID_ARG, "null context");
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  ctx->stats = dvg_stats{};
+  return DVG_OK;
+}
+
+static void validate_uploaded(dvg_context* ctx, dvg_matrix* m) {
+  reset_control(ctx);
+  launch_validate(ctx, m->rowmap, m->nrows, m->entries, m->nentries, m->ncols);
+  DeviceControl c = read_control(ctx);
+  if (c.invalid) {
+    std::string why;
+    if (c.invalid & 1) why += " rowmap[0] != 0;";
+    if (c.invalid & 2) why += " rowmap decreasing or odd row length;";
+    if (c.invalid & 4) why += " rowmap[nrows] != number of entries;";
+    if (c.invalid & 8) why += " column index >= ncols;";
+    throw Error(DVG_ERR_INVALID_ARG, "malformed range-CRS matrix:" + why);
+  }
+}
+
+static uint64_t count_nnz_host(const uint32_t* e, uint64_t n) {
+  uint64_t c = 0;
+  for (uint64_t i = 0; i + 1 < n; i += 2) c += uint64_t(e[i + 1]) - e[i] + 1;
+  return c;
+}
+
+dvg_status dvg_matrix_upload(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* rowmap,
+                             const uint32_t* entries, uint64_t nnz, dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(out && rowmap, "null argument");
+    require(ncols <= 0xFFFFFFFEu, "ncols must be below 2^32 - 1");
+    const uint64_t ne = rowmap[nrows];
+    require(ne == 0 || entries, "null entries");
+    dvg_matrix* m = new_matrix(ctx, nrows, ncols, ne);
+    try {
+      DVG_CUDA(cudaMemcpyAsync(m->rowmap, rowmap, (size_t(nrows) + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+      if (ne) DVG_CUDA(cudaMemcpyAsync(m->entries, entries, ne * 4, cudaMemcpyHostToDevice, ctx->stream));
+      ctx->stats.h2d_bytes += (uint64_t(nrows) + 1) * 8 + ne * 4;
+      validate_uploaded(ctx, m);
+      m->nnz = nnz ? nnz : count_nnz_host(entries, ne);
+    } catch (...) {
+      free_matrix(ctx, m);
+      throw;
+    }
+    *out = m;
+  });
+}
+
+dvg_status dvg_matrix_upload_u32(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint32_t* rowmap,
+                                 const uint32_t* entries, uint64_t nnz, dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(out && rowmap, "null argument");
+    require(ncols <= 0xFFFFFFFEu, "ncols must be below 2^32 - 1");
+    const uint64_t ne = rowmap[nrows];
+    require(ne == 0 || entries, "null entries");
+    dvg_matrix* m = new_matrix(ctx, nrows, ncols, ne);
+    uint32_t* tmp = nullptr;
+    try {
+      tmp = static_cast<uint32_t*>(dalloc(ctx, (size_t(nrows) + 1) * 4));
+      DVG_CUDA(cudaMemcpyAsync(tmp, rowmap, (size_t(nrows) + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+      launch_widen_rowmap(ctx, tmp, m->rowmap, uint64_t(nrows) + 1);
+      dfree(ctx, tmp);
+      tmp = nullptr;
+      if (ne) DVG_CUDA(cudaMemcpyAsync(m->entries, entries, ne * 4, cudaMemcpyHostToDevice, ctx->stream));
+      ctx->stats.h2d_bytes += (uint64_t(nrows) + 1) * 4 + ne * 4;
+      validate_uploaded(ctx, m);
+      m->nnz = nnz ? nnz : count_nnz_host(entries, ne);
+    } catch (...) {
+      if (tmp) dfree(ctx, tmp);
+      free_matrix(ctx, m);
+      throw;
+    }
+    *out = m;
+  });
+}
+
+dvg_status dvg_matrix_wrap_device(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* d_rowmap,
+                                  const uint32_t* d_entries, uint64_t nentries, uint64_t nnz, dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(out && d_rowmap && (nentries == 0 || d_entries), "null argument");
+    require(ncols <= 0xFFFFFFFEu, "ncols must be below 2^32 - 1");
+    require((reinterpret_cast<uintptr_t>(d_entries) & 7) == 0, "entries must be 8-byte aligned");
+    auto* m = new dvg_matrix();
+    m->nrows = nrows;
+    m->ncols = ncols;
+    m->nentries = nentries;
+    m->rowmap = const_cast<uint64_t*>(d_rowmap);
+    m->entries = const_cast<uint32_t*>(d_entries);
+    m->owned = false;
+    m->device = ctx->device;
+    try {
+      validate_uploaded(ctx, m);
+    } catch (...) {
+      delete m;
+      throw;
+    }
+    m->nnz = nnz;
+    *out = m;
+  });
+}
+
+dvg_status dvg_matrix_info(const dvg_matrix* m, uint32_t* nrows, uint32_t* ncols, uint64_t* nentries, uint64_t* nnz) {
+  if (!m) return fail(DVG_ERR_INVALID_ARG, "null matrix");
+  if (nrows) *nrows = m->nrows;
+  if (ncols) *ncols = m->ncols;
+  if (nentries) *nentries = m->nentries;
+  if (nnz) *nnz = m->nnz;
+  return DVG_OK;
+}
+
+dvg_status dvg_matrix_device_arrays(const dvg_matrix* m, const uint64_t** d_rowmap, const uint32_t** d_entries) {
+  if (!m) return fail(DVG_ERR_INVALID_ARG, "null matrix");
+  if (d_rowmap) *d_rowmap = m->rowmap;
+  if (d_entries) *d_entries = m->entries;
+  return DVG_OK;
+}
+
+dvg_status dvg_matrix_download(dvg_context* ctx, const dvg_matrix* m, uint64_t* rowmap, uint32_t* entries) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(m && rowmap && (m->nentries == 0 || entries), "null argument");
+    DVG_CUDA(cudaMemcpyAsync(rowmap, m->rowmap, (size_t(m->nrows) + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (m->nentries)
+      DVG_CUDA(cudaMemcpyAsync(entries, m->entries, m->nentries * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->stats.d2h_bytes += (uint64_t(m->nrows) + 1) * 8 + m->nentries * 4;
+    read_control(ctx);
+  });
+}
+
+dvg_status dvg_matrix_download_u32(dvg_context* ctx, const dvg_matrix* m, uint32_t* rowmap, uint32_t* entries) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(m && rowmap && (m->nentries == 0 || entries), "null argument");
+    if (m->nentries > 0xFFFFFFFFull) throw Error(DVG_ERR_OVERFLOW, "entries do not fit a 32-bit rowmap");
+    uint32_t* tmp = static_cast<uint32_t*>(dalloc(ctx, (size_t(m->nrows) + 1) * 4));
+    try {
+      launch_narrow_rowmap(ctx, m->rowmap, tmp, uint64_t(m->nrows) + 1);
+      DVG_CUDA(cudaMemcpyAsync(rowmap, tmp, (size_t(m->nrows) + 1) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+      if (m->nentries)
+        DVG_CUDA(cudaMemcpyAsync(entries, m->entries, m->nentries * 4, cudaMemcpyDeviceToHost, ctx->stream));
+      ctx->stats.d2h_bytes += (uint64_t(m->nrows) + 1) * 4 + m->nentries * 4;
+      read_control(ctx);
+    } catch (...) {
+      dfree(ctx, tmp);
+      throw;
+    }
+    dfree(ctx, tmp);
+  });
+}
+
+dvg_status dvg_matrix_free(dvg_context* ctx, dvg_matrix* m) {
+  if (!m) return DVG_OK;
+  return guarded([&] {
+    Lock lk(ctx);
+    free_matrix(ctx, m);
+  });
+}
+
+dvg_status dvg_range_identity(dvg_context* ctx, uint32_t n, dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(out != nullptr, "null output");
+    *out = identity(ctx, n);
+  });
+}
+
+dvg_status dvg_range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, dvg_matrix** c) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(a && b && c, "null argument");
+    *c = range_spadd(ctx, a, b, false);
+  });
+}
+
+dvg_status dvg_range_spgemm(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, dvg_matrix** c) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(a && b && c, "null argument");
+    dvg_matrix* r = range_spgemm(ctx, a, false, b);
+    try {
+      read_control(ctx);
+    } catch (...) {
+      free_matrix(ctx, r);
+      throw;
+    }
+    *c = r;
+  });
+}
+
+dvg_status dvg_range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k, dvg_matrix** c) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(a && c, "null argument");
+    dvg_matrix* r = range_power(ctx, a, k);
+    try {
+      read_control(ctx);
+    } catch (...) {
+      free_matrix(ctx, r);
+      throw;
+    }
+    *c = r;
+  });
+}
+
+dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, unsigned dmin, unsigned dmax,
+                                     dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(ra && out, "null argument");
+    dvg_matrix* r = create_distance_index(ctx, ra, dmin, dmax);
+    try {
+      read_control(ctx);
+    } catch (...) {
+      free_matrix(ctx, r);
+      throw;
+    }
+    *out = r;
+  });
+}
+
+dvg_status dvg_query_batch(dvg_context* ctx, const dvg_matrix* index, const uint32_t* d_pairs, uint64_t npairs,
+                           uint8_t* d_out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(index && (npairs == 0 || (d_pairs && d_out)), "null argument");
+    require((reinterpret_cast<uintptr_t>(d_pairs) & 7) == 0, "pairs must be 8-byte aligned");
+    reset_control(ctx);
+    launch_query(ctx, index, d_pairs, npairs, d_out);
+    DeviceControl c = read_control(ctx);
+    if (c.invalid) throw Error(DVG_ERR_INVALID_ARG, std::to_string(c.invalid) + " query pairs out of range");
+  });
+}
+
+dvg_status dvg_query_batch_host(dvg_context* ctx, const dvg_matrix* index, const uint32_t* pairs, uint64_t npairs,
+                                uint8_t* out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(index && (npairs == 0 || (pairs && out)), "null argument");
+    if (npairs == 0) return;
+    if (npairs > ctx->pairs_cap) {
+      if (ctx->d_pairs) dfree(ctx, ctx->d_pairs);
+      if (ctx->d_answers) dfree(ctx, ctx->d_answers);
+      ctx->d_pairs = nullptr;
+      ctx->d_answers = nullptr;
+      ctx->pairs_cap = 0;
+      ctx->d_pairs = static_cast<uint32_t*>(dalloc(ctx, npairs * 8));
+      ctx->d_answers = static_cast<uint8_t*>(dalloc(ctx, npairs));
+      ctx->pairs_cap = npairs;
+    }
+    DVG_CUDA(cudaMemcpyAsync(ctx->d_pairs, pairs, npairs * 8, cudaMemcpyHostToDevice, ctx->stream));
+    reset_control(ctx);
+    launch_query(ctx, index, ctx->d_pairs, npairs, ctx->d_answers);
+    DVG_CUDA(cudaMemcpyAsync(out, ctx->d_answers, npairs, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->stats.h2d_bytes += npairs * 8;
+    ctx->stats.d2h_bytes += npairs;
+    DeviceControl c = read_control(ctx);
+    if (c.invalid) throw Error(DVG_ERR_INVALID_ARG, std::to_string(c.invalid) + " query pairs out of range");
+  });
+}
+
+}  // extern "C"

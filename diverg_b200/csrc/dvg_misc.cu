@@ -1,0 +1,365 @@
+// dvg_misc.cu -- the streaming kernels of the path: identity, input
+// validation, rowmap width conversion, the rowmap scan, range SpAdd and the
+// batched membership query.
+#include <algorithm>
+
+#include "dvg_device.cuh"
+#include "dvg_internal.h"
+
+namespace dvg {
+namespace {
+
+constexpr int kThreads = 256;
+
+unsigned grid_for(dvg_context* ctx, uint64_t work, int per_block, int per_sm = 8) {
+  uint64_t want = (work + per_block - 1) / per_block;
+  uint64_t cap = uint64_t(ctx->num_sms) * per_sm;
+  return unsigned(std::max<uint64_t>(1, std::min(want, cap)));
+}
+
+// ---- identity: create_range_identity_matrix, range_sparse.hpp:66-88 -------
+__global__ void k_identity(uint64_t* __restrict__ rowmap, uint32_t* __restrict__ entries, uint32_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    reinterpret_cast<uint2*>(entries)[i] = make_uint2(uint32_t(i), uint32_t(i));
+    rowmap[i + 1] = 2 * (i + 1);
+    if (i == 0) rowmap[0] = 0;
+  }
+}
+
+// ---- validation: the memory-safety preconditions of every kernel ----------
+// bit 1: rowmap[0] != 0; bit 2: rowmap decreasing or odd row length;
+// bit 4: rowmap[n] != nentries; bit 8: an entry >= ncols.
+__global__ void k_validate(const uint64_t* __restrict__ rowmap, uint32_t nrows, const uint32_t* __restrict__ entries,
+                           uint64_t nentries, uint32_t ncols, DeviceControl* ctl) {
+  unsigned long long bad = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  for (uint64_t i = tid; i < nrows; i += stride) {
+    uint64_t a = rowmap[i], b = rowmap[i + 1];
+    if (b < a || ((b - a) & 1)) bad |= 2;
+  }
+  if (tid == 0) {
+    if (rowmap[0] != 0) bad |= 1;
+    if (rowmap[nrows] != nentries) bad |= 4;
+  }
+  for (uint64_t i = tid; i < nentries; i += stride)
+    if (entries[i] >= ncols) bad |= 8;
+  if (bad) atomicOr(&ctl->invalid, bad);
+}
+
+__global__ void k_widen(const uint32_t* __restrict__ src, uint64_t* __restrict__ dst, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+}
+
+__global__ void k_narrow(const uint64_t* __restrict__ src, uint32_t* __restrict__ dst, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    dst[i] = uint32_t(src[i]);
+}
+
+// ---- scan: rowmap[1..n] inclusive, in three passes (tile sums, tile
+// prefixes, apply) so no kernel waits on another CTA -------------------------
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kThreads * kScanItems;
+
+template <class T>
+__device__ T block_excl_scan(T v, T* warp_sums, T* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T u = __shfl_up_sync(kFullMask, incl, o);
+    if (lane >= o) incl += u;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  if (warp == 0) {
+    T s = lane < nw ? warp_sums[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T u = __shfl_up_sync(kFullMask, s, o);
+      if (lane >= o) s += u;
+    }
+    if (lane < nw) warp_sums[lane] = s;  // inclusive per warp
+  }
+  __syncthreads();
+  T base = warp ? warp_sums[warp - 1] : T(0);
+  if (total) *total = warp_sums[nw - 1];
+  T r = base + incl - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan_reduce(const uint64_t* __restrict__ data, uint64_t n,
+                                                          uint64_t* __restrict__ tile_sums) {
+  __shared__ uint64_t ws[32];
+  const uint64_t base = uint64_t(blockIdx.x) * kScanTile;
+  uint64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    uint64_t i = base + uint64_t(k) * kThreads + threadIdx.x;
+    if (i < n) s += data[i];
+  }
+  uint64_t total;
+  block_excl_scan<uint64_t>(s, ws, &total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(uint64_t* __restrict__ tile_sums, uint64_t nt) {
+  __shared__ uint64_t ws[32];
+  const uint64_t per = (nt + blockDim.x - 1) / blockDim.x;
+  const uint64_t b = threadIdx.x * per, e = std::min<uint64_t>(nt, b + per);
+  uint64_t s = 0;
+  for (uint64_t i = b; i < e; ++i) s += tile_sums[i];
+  uint64_t run = block_excl_scan<uint64_t>(s, ws, nullptr);
+  for (uint64_t i = b; i < e; ++i) {
+    uint64_t v = tile_sums[i];
+    tile_sums[i] = run;  // exclusive prefix of the tile
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_scan_apply(uint64_t* __restrict__ data, uint64_t n,
+                                                         const uint64_t* __restrict__ tile_prefix) {
+  __shared__ uint64_t tile[kScanTile];
+  __shared__ uint64_t ws[32];
+  const uint64_t base = uint64_t(blockIdx.x) * kScanTile;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    uint64_t i = base + uint64_t(k) * kThreads + threadIdx.x;
+    tile[k * kThreads + threadIdx.x] = i < n ? data[i] : 0;
+  }
+  __syncthreads();
+  uint64_t v[kScanItems];
+  uint64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    s += tile[threadIdx.x * kScanItems + k];
+    v[k] = s;
+  }
+  uint64_t pre = block_excl_scan<uint64_t>(s, ws, nullptr) + tile_prefix[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) tile[threadIdx.x * kScanItems + k] = v[k] + pre;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    uint64_t i = base + uint64_t(k) * kThreads + threadIdx.x;
+    if (i < n) data[i] = tile[k * kThreads + threadIdx.x];
+  }
+}
+
+// ---- SpAdd: range_spadd_symbolic / _numeric, range_sparse.hpp:145-224 and
+// :273-356.  One thread per row merges the two sorted range lists, merging a
+// range whose start is <= hi + 1 into the open one; after one list runs out
+// the other is merged up to its first non-merging range and copied verbatim
+// from there, exactly as the reference does. --------------------------------
+template <class Emit>
+__device__ __forceinline__ void spadd_row(const uint32_t* a, uint64_t na, const uint32_t* b, uint64_t nb,
+                                          Emit&& emit) {
+  uint64_t ai = 0, bi = 0;
+  if (ai < na && bi < nb) {
+    uint32_t lo, hi;
+    if (a[ai] <= b[bi]) { lo = a[ai]; hi = a[ai + 1]; ai += 2; }
+    else { lo = b[bi]; hi = b[bi + 1]; bi += 2; }
+    while (ai < na && bi < nb) {
+      uint32_t rs, re;
+      if (a[ai] <= b[bi]) { rs = a[ai]; re = a[ai + 1]; ai += 2; }
+      else { rs = b[bi]; re = b[bi + 1]; bi += 2; }
+      if (uint64_t(rs) <= uint64_t(hi) + 1) { lo = min(lo, rs); hi = max(hi, re); continue; }
+      emit(lo, hi);
+      lo = rs; hi = re;
+    }
+    while (ai < na || bi < nb) {
+      uint32_t rs, re;
+      if (ai == na) { rs = b[bi]; re = b[bi + 1]; bi += 2; }
+      else { rs = a[ai]; re = a[ai + 1]; ai += 2; }
+      if (uint64_t(rs) <= uint64_t(hi) + 1) { lo = min(lo, rs); hi = max(hi, re); continue; }
+      emit(lo, hi);
+      lo = rs; hi = re;
+      break;
+    }
+    emit(lo, hi);
+  }
+  for (; ai < na; ai += 2) emit(a[ai], a[ai + 1]);
+  for (; bi < nb; bi += 2) emit(b[bi], b[bi + 1]);
+}
+
+struct SpaddArgs {
+  const uint64_t* __restrict__ a_rowmap;
+  const uint32_t* __restrict__ a_entries;
+  const uint64_t* __restrict__ b_rowmap;
+  const uint32_t* __restrict__ b_entries;
+  uint64_t* __restrict__ c_rowmap;
+  uint32_t* __restrict__ c_entries;
+  DeviceControl* ctl;
+  uint32_t nrows;
+};
+
+template <bool B_IDENTITY, bool FILL>
+__global__ void __launch_bounds__(kThreads) k_spadd(SpaddArgs p) {
+  __shared__ unsigned long long cta_nnz;
+  if (threadIdx.x == 0) cta_nnz = 0;
+  __syncthreads();
+  unsigned long long my_nnz = 0;
+  for (uint64_t r = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; r < p.nrows;
+       r += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t a0 = p.a_rowmap[r], a1 = p.a_rowmap[r + 1];
+    uint32_t id[2] = {uint32_t(r), uint32_t(r)};
+    const uint32_t* b;
+    uint64_t nb;
+    if constexpr (B_IDENTITY) {
+      b = id;
+      nb = 2;
+    } else {
+      b = p.b_entries + p.b_rowmap[r];
+      nb = p.b_rowmap[r + 1] - p.b_rowmap[r];
+    }
+    if constexpr (FILL) {
+      uint64_t pos = p.c_rowmap[r];
+      const uint64_t end = p.c_rowmap[r + 1];
+      spadd_row(p.a_entries + a0, a1 - a0, b, nb, [&](uint32_t lo, uint32_t hi) {
+        if (pos + 2 <= end) {
+          p.c_entries[pos] = lo;
+          p.c_entries[pos + 1] = hi;
+        } else {
+          atomicOr(&p.ctl->status, 4ull);
+        }
+        pos += 2;
+      });
+    } else {
+      uint64_t cnt = 0;
+      spadd_row(p.a_entries + a0, a1 - a0, b, nb, [&](uint32_t lo, uint32_t hi) {
+        cnt += 2;
+        my_nnz += uint64_t(hi) - lo + 1;
+      });
+      p.c_rowmap[r + 1] = cnt;
+    }
+  }
+  if constexpr (!FILL) {
+    atomicAdd(&cta_nnz, my_nnz);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&p.ctl->nnz, cta_nnz);
+  }
+}
+
+// ---- query: crs_matrix::binary_search(..., RangeGroup), crs_matrix.hpp:
+// 149-169, one thread per pair ------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_query(const uint64_t* __restrict__ rowmap,
+                                                    const uint32_t* __restrict__ entries, uint32_t nrows,
+                                                    uint32_t ncols, const uint2* __restrict__ pairs, uint64_t npairs,
+                                                    uint8_t* __restrict__ out, DeviceControl* ctl) {
+  unsigned long long bad = 0;
+  for (uint64_t q = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; q < npairs;
+       q += uint64_t(gridDim.x) * blockDim.x) {
+    uint2 ij = pairs[q];
+    uint8_t ans = 0;
+    if (ij.x < nrows && ij.y < ncols) {
+      const uint64_t lo = __ldg(rowmap + ij.x), hi = __ldg(rowmap + ij.x + 1);
+      uint64_t first = lo, len = hi - lo;
+      while (len > 0) {
+        uint64_t half = len >> 1;
+        if (__ldg(entries + first + half) < ij.y) {
+          first += half + 1;
+          len -= half + 1;
+        } else {
+          len = half;
+        }
+      }
+      if ((first - lo) & 1) --first;
+      ans = (first != hi && __ldg(entries + first) <= ij.y) ? 1 : 0;
+    } else {
+      ++bad;
+    }
+    out[q] = ans;
+  }
+  if (bad) atomicAdd(&ctl->invalid, bad);
+}
+
+}  // namespace
+
+void launch_identity(dvg_context* ctx, dvg_matrix* out) {
+  if (out->nrows == 0) {
+    DVG_CUDA(cudaMemsetAsync(out->rowmap, 0, sizeof(uint64_t), ctx->stream));
+    return;
+  }
+  k_identity<<<grid_for(ctx, out->nrows, kThreads), kThreads, 0, ctx->stream>>>(out->rowmap, out->entries,
+                                                                                out->nrows);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+void launch_validate(dvg_context* ctx, const uint64_t* rowmap, uint32_t nrows, const uint32_t* entries,
+                     uint64_t nentries, uint32_t ncols) {
+  k_validate<<<grid_for(ctx, std::max<uint64_t>(nrows, nentries) + 1, kThreads), kThreads, 0, ctx->stream>>>(
+      rowmap, nrows, entries, nentries, ncols, ctx->d_ctl);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+void launch_widen_rowmap(dvg_context* ctx, const uint32_t* src, uint64_t* dst, uint64_t n) {
+  k_widen<<<grid_for(ctx, n, kThreads), kThreads, 0, ctx->stream>>>(src, dst, n);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+void launch_narrow_rowmap(dvg_context* ctx, const uint64_t* src, uint32_t* dst, uint64_t n) {
+  k_narrow<<<grid_for(ctx, n, kThreads), kThreads, 0, ctx->stream>>>(src, dst, n);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+void launch_rowmap_scan(dvg_context* ctx, uint64_t* rowmap, uint64_t n) {
+  if (n == 0) return;
+  uint64_t* data = rowmap + 1;
+  const uint64_t nt = (n + kScanTile - 1) / kScanTile;
+  if (nt > ctx->tile_sums_cap) {
+    if (ctx->d_tile_sums) dfree(ctx, ctx->d_tile_sums);
+    ctx->d_tile_sums = nullptr;
+    ctx->tile_sums_cap = 0;
+    ctx->d_tile_sums = static_cast<uint64_t*>(dalloc(ctx, nt * sizeof(uint64_t)));
+    ctx->tile_sums_cap = nt;
+  }
+  k_scan_reduce<<<unsigned(nt), kThreads, 0, ctx->stream>>>(data, n, ctx->d_tile_sums);
+  DVG_CUDA(cudaGetLastError());
+  k_scan_tiles<<<1, 1024, 0, ctx->stream>>>(ctx->d_tile_sums, nt);
+  DVG_CUDA(cudaGetLastError());
+  k_scan_apply<<<unsigned(nt), kThreads, 0, ctx->stream>>>(data, n, ctx->d_tile_sums);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches += 3;
+}
+
+void launch_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity, uint64_t* c_rowmap,
+                  uint32_t* c_entries, bool fill) {
+  if (a->nrows == 0) return;
+  SpaddArgs p{};
+  p.a_rowmap = a->rowmap;
+  p.a_entries = a->entries;
+  p.b_rowmap = b_identity ? nullptr : b->rowmap;
+  p.b_entries = b_identity ? nullptr : b->entries;
+  p.c_rowmap = c_rowmap;
+  p.c_entries = c_entries;
+  p.ctl = ctx->d_ctl;
+  p.nrows = a->nrows;
+  const unsigned grid = grid_for(ctx, a->nrows, kThreads);
+  if (b_identity) {
+    if (fill) k_spadd<true, true><<<grid, kThreads, 0, ctx->stream>>>(p);
+    else k_spadd<true, false><<<grid, kThreads, 0, ctx->stream>>>(p);
+  } else {
+    if (fill) k_spadd<false, true><<<grid, kThreads, 0, ctx->stream>>>(p);
+    else k_spadd<false, false><<<grid, kThreads, 0, ctx->stream>>>(p);
+  }
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out) {
+  if (npairs == 0) return;
+  k_query<<<grid_for(ctx, npairs, kThreads, 16), kThreads, 0, ctx->stream>>>(
+      idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint2*>(d_pairs), npairs, d_out,
+      ctx->d_ctl);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+}  // namespace dvg

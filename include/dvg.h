@@ -1,0 +1,143 @@
+/*
+ * dvg.h -- C ABI of libdvg.so: DiVerG's distance-index path on one B200.
+ *
+ * Plain C, plain pointers and sizes.  Every entry point returns a dvg_status;
+ * dvg_last_error() gives a message for the last failure of the calling thread.
+ * The C++ headers under include/diverg/ wrap this ABI in the reference's own
+ * API (CRSMatrix<RangeDynamic,...>, range_spgemm, create_distance_index, ...);
+ * each declaration below names the reference interface (file:line in
+ * cartoonist/diverg v1.1.1) it stands in for.
+ *
+ * Matrices are range CRS, as CRSMatrix<crs_matrix::RangeDynamic, bool,
+ * uint32_t, TSize> (include/diverg/crs_matrix.hpp:1873-2004):
+ *   rowmap  : TSize[nrows+1] counting ENTRIES (two per range), rowmap[0] = 0
+ *   entries : uint32_t[rowmap[nrows]], inclusive [start,end] pairs, sorted
+ *   nnz     : number of non-zero columns, sum of (end - start + 1)
+ * A dvg_matrix lives in device memory (HBM) until dvg_matrix_free.
+ *
+ * Threading: calls on one context are serialised by the context; distinct
+ * contexts may be used from distinct threads.  All work of a context is
+ * issued on its stream; calls that return sizes or status to the host
+ * synchronise that stream.
+ */
+#ifndef DVG_H
+#define DVG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum dvg_status {
+  DVG_OK = 0,
+  DVG_ERR_INVALID_ARG = 1,   /* bad argument (the reference asserts / exits 134) */
+  DVG_ERR_OOM = 2,           /* device or pinned host allocation failed */
+  DVG_ERR_DEVICE = 3,        /* CUDA error, or no usable sm_100 device */
+  DVG_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up */
+  DVG_ERR_NOT_INITIALIZED = 5,
+  DVG_ERR_OVERFLOW = 6       /* result does not fit the requested index type */
+} dvg_status;
+
+typedef struct dvg_context dvg_context;
+typedef struct dvg_matrix dvg_matrix;
+
+/* Counters of the work a context issued since its creation or the last
+ * dvg_stats_reset. */
+typedef struct dvg_stats {
+  uint64_t kernel_launches;   /* kernels of this library launched */
+  uint64_t spgemm_calls;      /* range SpGEMM products */
+  uint64_t spadd_calls;       /* range SpAdd sums */
+  uint64_t host_syncs;        /* stream synchronisations for size read-backs */
+  uint64_t alg_bytes;         /* compulsory bytes: read A and B once, write C once */
+  uint64_t spgemm_alg_bytes;  /* the share of alg_bytes due to SpGEMM */
+  uint64_t range_ops;         /* B ranges visited by SpGEMM (work metric) */
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  /* device time of the kernels, measured with CUDA events on the context's
+   * stream while the "timing" option is on (0 otherwise) */
+  uint64_t spgemm_symbolic_ns;  /* SpGEMM symbolic passes */
+  uint64_t spgemm_numeric_ns;   /* SpGEMM numeric passes */
+  uint64_t scan_ns;             /* rowmap scans (SpGEMM and SpAdd) */
+  uint64_t spadd_ns;            /* SpAdd passes */
+} dvg_stats;
+
+/* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /
+ *      ScopedRuntime) and src/eti/runtime.cpp ------------------------------ */
+
+/* Opens `device` (a CUDA ordinal), checks it is an sm_100 part and creates a
+ * context with its own non-blocking stream. */
+dvg_status dvg_init(int device, dvg_context** ctx);
+/* Waits for the context's work, frees its scratch and destroys the stream if
+ * the context owns it.  Matrices must be freed before. */
+dvg_status dvg_shutdown(dvg_context* ctx);
+/* Issue the context's work on a caller-owned cudaStream_t (NULL restores the
+ * context's own stream). */
+dvg_status dvg_set_stream(dvg_context* ctx, void* cuda_stream);
+dvg_status dvg_synchronize(dvg_context* ctx);
+/* Tuning knobs: "group_lanes" (0 = autotune, or 4/8/16/32 lanes per output
+ * row), "window_words" (0 = default, else 32-bit words of accumulator per row
+ * group), "timing" (1 = time kernels with CUDA events into dvg_stats). */
+dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value);
+dvg_status dvg_get_stats(const dvg_context* ctx, dvg_stats* out);
+dvg_status dvg_stats_reset(dvg_context* ctx);
+const char* dvg_last_error(void);
+const char* dvg_status_string(dvg_status s);
+
+/* ---- matrices: crs_matrix_device.hpp:192-238 (entries_device_view /
+ *      rowmap_device_view, H2D) and :265-290 (make_crs_matrix, D2H) -------- */
+
+/* Copies a host range-CRS matrix to the device.  nnz may be 0, in which case
+ * it is recounted (CRSMatrix ctor, crs_matrix.hpp:1894-1902). */
+dvg_status dvg_matrix_upload(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* rowmap,
+                             const uint32_t* entries, uint64_t nnz, dvg_matrix** out);
+/* Same with a 32-bit rowmap (CRSMatrix<..., uint32_t, uint32_t>). */
+dvg_status dvg_matrix_upload_u32(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint32_t* rowmap,
+                                 const uint32_t* entries, uint64_t nnz, dvg_matrix** out);
+/* Wraps caller-owned device arrays without copying; the arrays must outlive
+ * the handle and are not freed by dvg_matrix_free. */
+dvg_status dvg_matrix_wrap_device(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* d_rowmap,
+                                  const uint32_t* d_entries, uint64_t nentries, uint64_t nnz, dvg_matrix** out);
+/* numRows / numCols / rowMap(numRows) / nnz (crs_matrix.hpp:1274-1369, 1980). */
+dvg_status dvg_matrix_info(const dvg_matrix* m, uint32_t* nrows, uint32_t* ncols, uint64_t* nentries, uint64_t* nnz);
+dvg_status dvg_matrix_device_arrays(const dvg_matrix* m, const uint64_t** d_rowmap, const uint32_t** d_entries);
+/* Copies to caller buffers of nrows+1 and nentries elements. */
+dvg_status dvg_matrix_download(dvg_context* ctx, const dvg_matrix* m, uint64_t* rowmap, uint32_t* entries);
+dvg_status dvg_matrix_download_u32(dvg_context* ctx, const dvg_matrix* m, uint32_t* rowmap, uint32_t* entries);
+dvg_status dvg_matrix_free(dvg_context* ctx, dvg_matrix* m);
+
+/* ---- range operations: include/diverg/range_sparse.hpp ------------------- */
+
+/* create_range_identity_matrix<RCRS>(n), range_sparse.hpp:95-110. */
+dvg_status dvg_range_identity(dvg_context* ctx, uint32_t n, dvg_matrix** out);
+/* range_spadd(a, b), range_sparse.hpp:470-477 (-> :364-428, :112-357). */
+dvg_status dvg_range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, dvg_matrix** c);
+/* range_spgemm(a, b, config), range_sparse.hpp:2325-2332 (-> :2215-2281). */
+dvg_status dvg_range_spgemm(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, dvg_matrix** c);
+/* range_power(a, k, config), range_sparse.hpp:2362-2368 (-> :2370-2431). */
+dvg_status dvg_range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k, dvg_matrix** c);
+
+/* ---- distance index: dindex.hpp:46-189, dindex_eti.hpp:44-53 ------------- */
+
+/* create_distance_index(ra, dmin, dmax): A^dmin * (A+I)^(dmax-dmin).
+ * Requires dmin <= dmax, dmax != 0 and a square `ra`. */
+dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, unsigned dmin, unsigned dmax,
+                                     dvg_matrix** out);
+
+/* ---- membership query: crs_matrix.hpp:1197-1243 (operator() / at) -------- */
+
+/* out[q] = index(pairs[2q], pairs[2q+1]) as 0/1 for q < npairs; device
+ * pointers.  Pairs outside [0,nrows) x [0,ncols) answer 0 and make the call
+ * return DVG_ERR_INVALID_ARG (at() throws std::runtime_error there). */
+dvg_status dvg_query_batch(dvg_context* ctx, const dvg_matrix* index, const uint32_t* d_pairs, uint64_t npairs,
+                           uint8_t* d_out);
+/* The same with host buffers (copies in and out on the context's stream). */
+dvg_status dvg_query_batch_host(dvg_context* ctx, const dvg_matrix* index, const uint32_t* pairs, uint64_t npairs,
+                                uint8_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DVG_H */

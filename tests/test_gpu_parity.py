@@ -1,0 +1,237 @@
+"""Parity of the sm_100a path (through the C ABI of libdvg.so) with the CPU
+oracle and the golden fixtures.  Integer work: every comparison is exact."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as orc
+from diverg_b200 import CRSMatrix, _native as N, gen
+from diverg_b200.runtime import Context
+from tests.conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+# group sizes x accumulator windows: "auto", every group size at its default
+# window, and tiny windows that force the multi-chunk path
+PLANS = [(0, 0), (4, 0), (8, 0), (16, 0), (32, 0), (4, 1), (8, 3), (32, 2), (16, 37)]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def set_plan(ctx, plan):
+    ctx.set_option("group_lanes", plan[0])
+    ctx.set_option("window_words", plan[1])
+
+
+def as_crs(o):
+    return CRSMatrix(o.ncols, o.entries, o.rowmap, o.nnz)
+
+
+def omat(m):
+    return orc.OMat(m.numRows(), m.numCols(), m.rowmap.astype(np.uint64), m.entries, m.nnz())
+
+
+def assert_same(got: CRSMatrix, rowmap, entries, nnz, what=""):
+    assert np.array_equal(got.rowmap.astype(np.uint64), np.asarray(rowmap, np.uint64)), what
+    assert np.array_equal(got.entries, np.asarray(entries, np.uint32)), what
+    assert got.nnz() == int(nnz), what
+
+
+@pytest.mark.parametrize("plan", PLANS)
+def test_hbitvector_known_answer(ctx, plan):
+    # test_hbitvector.cpp:186-234 -> :618-661: I * A canonicalises A's rows
+    set_plan(ctx, plan)
+    ki = load_golden("hbv_known_answer.npz")
+    a = ctx.upload(CRSMatrix(int(ki["ncols"]), ki["in_entries"], ki["in_rowmap"]))
+    i5 = ctx.identity(5)
+    c = ctx.spgemm(i5, a).download()
+    assert_same(c, ki["out_rowmap"], ki["out_entries"], orc.nnz(orc.OMat(5, 11431, ki["out_rowmap"],
+                                                                          ki["out_entries"], 0)))
+
+
+@pytest.mark.parametrize("name", ["x", "multi", "m"])
+@pytest.mark.parametrize("plan", [(0, 0), (4, 0), (32, 0), (8, 3)])
+def test_gfa_fixture_products(ctx, name, plan):
+    set_plan(ctx, plan)
+    g = load_golden(f"gfa_{name}.npz")
+    n = int(g["n"])
+    A = CRSMatrix(n, g["A_entries"], g["A_rowmap"], int(g["A_nnz"]))
+    dA = ctx.upload(A)
+    for key in [k[:-7] for k in g if k.endswith("_rowmap") and k != "A_rowmap"]:
+        if key == "AA":
+            r = ctx.spgemm(dA, dA)
+        elif key == "AI":
+            r = ctx.spadd(dA, ctx.identity(n))
+        elif key.startswith("P"):
+            r = ctx.power(dA, int(key[1:]))
+        else:
+            lo, hi = map(int, key[1:].split("_"))
+            r = ctx.distance_index(dA, lo, hi)
+        assert_same(r.download(), g[key + "_rowmap"], g[key + "_entries"], g[key + "_nnz"], f"{name} {key}")
+
+
+@pytest.mark.parametrize("plan", PLANS)
+def test_random_spgemm_reference_shape(ctx, plan):
+    # test_range_sparse.cpp:516-520: N = 6521, NNZ = 200000, A * A
+    set_plan(ctx, plan)
+    a = gen.random_matrix(6521, 200000, seed=21)
+    want = orc.spgemm(omat(a), omat(a), algo="hbv")
+    da = ctx.upload(a)
+    assert_same(ctx.spgemm(da, da).download(), want.rowmap, want.entries, want.nnz)
+
+
+@pytest.mark.parametrize("plan", [(0, 0), (4, 0), (16, 0), (8, 5)])
+def test_random_power_reference_shape(ctx, plan):
+    # test_range_sparse.cpp:590-594: N = 6521, NNZ = 4000, K = 100
+    set_plan(ctx, plan)
+    a = gen.random_matrix(6521, 4000, seed=22)
+    want = orc.power(omat(a), 100, algo="hbv")
+    assert_same(ctx.power(ctx.upload(a), 100).download(), want.rowmap, want.entries, want.nnz)
+
+
+@pytest.mark.parametrize("n,nnz", [(6521, 4000), (20, 220), (5000, 300000)])
+def test_random_spadd_reference_shapes(ctx, n, nnz):
+    # test_range_sparse.cpp:664-665
+    a = gen.random_matrix(n, nnz, seed=23)
+    b = gen.random_matrix(n, nnz, seed=24)
+    want = orc.spadd(omat(a), omat(b))
+    assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
+
+
+def test_rectangular_spgemm(ctx):
+    set_plan(ctx, (0, 0))
+    a = gen.random_matrix(3000, 30000, seed=5)
+    b = gen.banded(3000, 64, 3.0, 16.0, seed=6)
+    # a: 3000 x 3000, b: 3000 x 3000 -> check A*B and B*A
+    for x, y in ((a, b), (b, a)):
+        want = orc.spgemm(omat(x), omat(y))
+        assert_same(ctx.spgemm(ctx.upload(x), ctx.upload(y)).download(), want.rowmap, want.entries, want.nnz)
+
+
+@pytest.mark.parametrize("plan", [(0, 0), (8, 0), (32, 4)])
+def test_banded_spgemm(ctx, plan):
+    set_plan(ctx, plan)
+    a = gen.banded(1 << 16, 512, 4.0, 32.0, seed=31)
+    b = gen.banded(1 << 16, 512, 4.0, 32.0, seed=32)
+    want = orc.spgemm(omat(a), omat(b), algo="hbv")
+    assert_same(ctx.spgemm(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
+    want = orc.spadd(omat(a), omat(b))
+    assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
+
+
+@pytest.mark.parametrize("window", [(100, 300), (0, 250), (150, 450), (1, 1), (7, 7), (0, 1)])
+def test_small_graph_index(ctx, window):
+    set_plan(ctx, (0, 0))
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(100_000, seed=42))
+    want = orc.dindex(omat(a), window[0], window[1], algo="hbv")
+    got = ctx.distance_index(ctx.upload(a), *window).download()
+    assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
+
+
+def test_graph_with_structural_bubbles_index(ctx):
+    set_plan(ctx, (0, 0))
+    spec = gen.GraphSpec(60_000, 1e-3, 2e-4, 0.5, 1, 50, 4.0, 0.05, 100, 2000, seed=8)
+    a, st = gen.graph_adjacency(spec)
+    assert st["n_sv"] > 0
+    want = orc.dindex(omat(a), 400, 600, algo="hbv")
+    got = ctx.distance_index(ctx.upload(a), 400, 600).download()
+    assert_same(got, want.rowmap, want.entries, want.nnz)
+
+
+def test_query_batch_matches_oracle(ctx):
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(50_000, seed=4))
+    idx = orc.dindex(omat(a), 100, 300, algo="hbv")
+    d_idx = ctx.upload(as_crs(idx))
+    pairs = gen.query_pairs(a, 200_000, 0.5, 100, 300, seed=3)
+    want = orc.query(idx, pairs)
+    got = ctx.query(d_idx, pairs)
+    assert np.array_equal(got, want)
+    assert want.sum() > 50_000  # the in-range half mostly hits
+
+
+def test_query_rejects_out_of_range_pairs(ctx):
+    d = ctx.identity(10)
+    with pytest.raises(N.DvgError) as e:
+        ctx.query(d, np.array([[1, 1], [10, 2]], np.uint32))
+    assert e.value.status == N.INVALID_ARG
+
+
+def test_u32_rowmap_overload(ctx):
+    # dindex_eti.hpp:50-53: the <uint32_t, uint32_t> overload
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(30_000, seed=9))
+    want = orc.dindex(omat(a), 1, 8)
+    a32 = CRSMatrix(a.numCols(), a.entries, a.rowmap.astype(np.uint32), a.nnz(), size_type=np.uint32)
+    got = ctx.distance_index(ctx.upload(a32), 1, 8).download(np.uint32)
+    assert got.rowmap.dtype == np.uint32
+    assert_same(got, want.rowmap, want.entries, want.nnz)
+
+
+def test_edge_cases(ctx):
+    # empty matrix, empty rows, a row whose runs end on 32-bit word edges, and
+    # columns at the top of the uint32 range
+    z = ctx.upload(CRSMatrix(0, np.zeros(0, np.uint32), np.zeros(1, np.uint64)))
+    assert ctx.spgemm(z, z).download().numRows() == 0
+    e = CRSMatrix(5, np.zeros(0, np.uint32), np.zeros(6, np.uint64))
+    de = ctx.upload(e)
+    assert ctx.spgemm(de, de).download().entries.size == 0
+    assert ctx.power(de, 3).download().entries.size == 0
+    ent = np.array([0, 31, 32, 32, 63, 63, 95, 127, 160, 191], np.uint32)
+    b = CRSMatrix(256, ent, np.array([0, len(ent)], np.uint64))
+    for plan in PLANS:
+        set_plan(ctx, plan)
+        c = ctx.spgemm(ctx.identity(1), ctx.upload(b)).download()
+        assert list(c.entries) == [0, 32, 63, 63, 95, 127, 160, 191], plan
+    top = 0xFFFFFFFE
+    hi = np.array([top - 70, top - 40, top - 33, top - 1], np.uint32)
+    B = CRSMatrix(top, hi, np.array([0, 2, 4, 4], np.uint64))
+    A = CRSMatrix(3, np.array([0, 1, 1, 2, 0, 0], np.uint32), np.array([0, 2, 4, 6], np.uint64))
+    want = orc.spgemm(omat(A), omat(B))
+    for plan in PLANS:
+        set_plan(ctx, plan)
+        assert_same(ctx.spgemm(ctx.upload(A), ctx.upload(B)).download(), want.rowmap, want.entries, want.nnz,
+                    str(plan))
+
+
+def test_errors_are_reported(ctx):
+    a = ctx.identity(4)
+    b = ctx.identity(5)
+    with pytest.raises(N.DvgError) as e:
+        ctx.spgemm(a, b)
+    assert e.value.status == N.INVALID_ARG
+    with pytest.raises(N.DvgError) as e:
+        ctx.distance_index(a, 3, 2)
+    assert e.value.status == N.INVALID_ARG
+    with pytest.raises(N.DvgError) as e:
+        ctx.distance_index(a, 0, 0)
+    assert e.value.status == N.INVALID_ARG
+    bad = CRSMatrix(4, np.array([0, 9], np.uint32), np.array([0, 2, 2, 2, 2], np.uint64))
+    with pytest.raises(N.DvgError) as e:
+        ctx.upload(bad)
+    assert e.value.status == N.INVALID_ARG
+    odd = CRSMatrix(4, np.array([0, 1, 2], np.uint32), np.array([0, 3, 3, 3, 3], np.uint64), 1)
+    with pytest.raises(N.DvgError):
+        ctx.upload(odd)
+
+
+def test_reference_api_mirror():
+    import diverg_b200 as dv
+    with dv.ScopedRuntime():
+        a, _ = gen.graph_adjacency(gen.small_graph_spec(20_000, seed=1))
+        idx = dv.create_distance_index(a, 10, 30)
+        want = orc.dindex(omat(a), 10, 30)
+        assert_same(idx, want.rowmap, want.entries, want.nnz)
+        sq = dv.range_spgemm(a, a)
+        want = orc.spgemm(omat(a), omat(a))
+        assert_same(sq, want.rowmap, want.entries, want.nnz)
+        ai = dv.range_spadd(a, dv.create_range_identity_matrix(a.numRows()))
+        want = orc.spadd(omat(a), orc.identity(a.numRows()))
+        assert_same(ai, want.rowmap, want.entries, want.nnz)
+        p = dv.range_power(a, 5)
+        want = orc.power(omat(a), 5)
+        assert_same(p, want.rowmap, want.entries, want.nnz)
+        pairs = gen.query_pairs(a, 1000, 0.5, 10, 30)
+        assert np.array_equal(dv.query_batch(idx, pairs), orc.query(omat(idx), pairs))
