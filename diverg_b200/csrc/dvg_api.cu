@@ -1,6 +1,7 @@
 // dvg_api.cu -- the C ABI of include/dvg.h and the host orchestration of the
 // range operations: products, sums, powers and the distance index.  Every
 // entry point converts internal failures into a dvg_status.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -165,8 +166,47 @@ static DeviceControl read_total(dvg_context* ctx, const uint64_t* rowmap_last, u
   return c;
 }
 
+static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b) {
+  const uint32_t n = a_identity ? b->nrows : a->nrows;
+  // speculative output capacity; an overflow is detected and re-run exactly
+  const uint64_t a_ent = a_identity ? 2ull * n : a->nentries;
+  uint64_t cap = std::max<uint64_t>({2 * a_ent, 2 * b->nentries, 4ull * n, 64});
+  dvg_matrix* c = new_matrix(ctx, n, b->ncols, cap);
+  try {
+    DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
+    DeviceControl ctl{};
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      reset_control(ctx);
+      cudaEvent_t t0 = span_begin(ctx);
+      launch_spgemm_fused(ctx, a, a_identity, b, c->rowmap, c->entries, cap);
+      span_end(ctx, t0, kSymbolic);
+      ctl = read_control(ctx);
+      if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "range_spgemm: tile look-back wait expired");
+      if (!ctl.overflow) break;
+      if (attempt == 1) throw Error(DVG_ERR_DEVICE, "range_spgemm: output capacity overflow after resize");
+      ctx->stats.spgemm_reruns++;
+      cap = ctl.total;
+      dfree(ctx, c->entries);
+      c->entries = nullptr;
+      c->entries = static_cast<uint32_t*>(dalloc(ctx, entries_alloc_bytes(cap)));
+    }
+    c->nentries = ctl.total;
+    c->nnz = ctl.nnz;
+    ctx->stats.spgemm_calls++;
+    ctx->stats.spgemm_direct_tiles += ctl.tiles_direct;
+    uint64_t bytes = (a_identity ? 0 : matrix_bytes(a)) + matrix_bytes(b) + matrix_bytes(c);
+    ctx->stats.alg_bytes += bytes;
+    ctx->stats.spgemm_alg_bytes += bytes;
+  } catch (...) {
+    free_matrix(ctx, c);
+    throw;
+  }
+  return c;
+}
+
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b) {
   if (!a_identity) require(a->ncols == b->nrows, "range_spgemm: a.numCols() != b.numRows()");
+  if (ctx->opt_algo == 0) return range_spgemm_fused(ctx, a, a_identity, b);
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   dvg_matrix* c = new_matrix(ctx, n, b->ncols, 0);
   try {
@@ -378,6 +418,8 @@ dvg_status dvg_shutdown(dvg_context* ctx) {
     if (ctx->d_tile_sums) dfree(ctx, ctx->d_tile_sums);
     if (ctx->d_pairs) dfree(ctx, ctx->d_pairs);
     if (ctx->d_answers) dfree(ctx, ctx->d_answers);
+    if (ctx->d_tile_desc) dfree(ctx, ctx->d_tile_desc);
+    if (ctx->d_ticket) dfree(ctx, ctx->d_ticket);
     DVG_CUDA(cudaStreamSynchronize(ctx->stream));
     resolve_spans(ctx);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
@@ -417,6 +459,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "window_words")) {
       require(value >= 0 && value <= 4096, "window_words must be in [0, 4096]");
       ctx->opt_window_words = value;
+    } else if (!std::strcmp(key, "algo")) {
+      require(value == 0 || value == 1, "algo must be 0 (fused tiled) or 1 (two-pass direct)");
+      ctx->opt_algo = value;
     } else if (!std::strcmp(key, "timing")) {
       DVG_CUDA(cudaStreamSynchronize(ctx->stream));
       resolve_spans(ctx);

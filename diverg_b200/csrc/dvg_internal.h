@@ -29,6 +29,10 @@ struct DeviceControl {
   unsigned long long range_ops;  // B ranges visited by the last product
   unsigned long long invalid;    // query pairs out of range / validation bits
   unsigned long long status;     // nonzero: a kernel detected an internal error
+  unsigned long long total;      // entries of the last fused product
+  unsigned long long overflow;   // nonzero: the fused product exceeded its capacity
+  unsigned long long timeout;    // nonzero: a bounded device wait gave up
+  unsigned long long tiles_direct;  // tiles that took the direct (unstaged) path
 };
 
 struct dvg_context {
@@ -42,11 +46,15 @@ struct dvg_context {
   DeviceControl* h_ctl = nullptr;     // pinned host mirror
   uint64_t* d_tile_sums = nullptr;    // scan scratch
   size_t tile_sums_cap = 0;
+  void* d_tile_desc = nullptr;        // fused SpGEMM look-back descriptors
+  size_t tile_desc_cap = 0;           // bytes
+  unsigned* d_ticket = nullptr;       // fused SpGEMM tile ticket
   uint32_t* d_pairs = nullptr;        // staging for host-buffer queries
   uint8_t* d_answers = nullptr;
   uint64_t pairs_cap = 0;
   int64_t opt_group_lanes = 0;
   int64_t opt_window_words = 0;
+  int64_t opt_algo = 0;               // 0: fused tiled SpGEMM, 1: two-pass direct
   bool opt_timing = false;
   // event pairs bracketing timed kernels, resolved at the next stream sync
   struct TimedSpan {
@@ -108,6 +116,12 @@ SpgemmPlan plan_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, c
 // b->nrows and `a` is ignored.
 void launch_spgemm(dvg_context* ctx, const SpgemmPlan& plan, const dvg_matrix* a, bool a_identity,
                    const dvg_matrix* b, uint64_t* c_rowmap, uint32_t* c_entries, bool fill);
+
+// Fused single-pass SpGEMM (dvg_spgemm_fused.cu): writes c_rowmap fully and
+// c_entries up to `cap` entries; the control block receives the total entry
+// count, the nnz and an overflow flag when total > cap.
+void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
+                         uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap);
 
 // Host orchestration (dvg_api.cu).
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b);

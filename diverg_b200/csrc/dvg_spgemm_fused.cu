@@ -1,0 +1,694 @@
+// dvg_spgemm_fused.cu -- single-pass, tile-staged range SpGEMM C = A*B.
+//
+// Same result as the reference's symbolic + numeric SpGEMM
+// (include/diverg/range_sparse.hpp:1132-1442 in cartoonist/diverg, the
+// TeamSequential / HBitVector pair, dispatched by range_spgemm :2215-2281):
+// row r of C is the union of all ranges of B rows s..f for every range
+// [s,f] of A's row r, emitted as sorted maximal runs.
+//
+// The kernel is persistent: each CTA takes tiles of kTileRows consecutive C
+// rows from an atomic ticket, so tiles start in order, and
+//  1. stages the tile's A ranges and the slice of B rows they name (one
+//     contiguous rowmap window and one contiguous entries window) in shared
+//     memory;
+//  2. builds, over the staged B rows, union bitmaps on the tile's column
+//     window: for blocks of `sb` rows, the prefix union PRE[j] (block start
+//     .. j), the suffix union SUF[j] (j .. block end) and the block union
+//     BU[b].  A range [s,f] of A then costs SUF[s] | BU[..] | PRE[f] -- a few
+//     word ORs per column word -- instead of one visit per B row, which is
+//     what dominates products of wide-range matrices (powers of A+I);
+//  3. gathers every C row from those words with the boundary masks of the
+//     reference's HBitVector gather (map01 / map10, hbitvector.hpp:568-597):
+//     popc counts, a lane-group prefix sum places, ffs extracts;
+//  4. stages the row runs in shared memory, obtains the tile's output offset
+//     by decoupled look-back over the tile ticket order (no separate
+//     symbolic pass or scan kernel), then writes c_rowmap and c_entries
+//     with coalesced stores.
+// Tiles whose A ranges, B slice or column window exceed the staging buffers
+// take the direct path: a warp per row accumulates the B ranges in a shared
+// bitvector window (column chunks when the band is wider), counts, joins the
+// look-back, then recomputes and writes.  Look-back waits are bounded; on
+// expiry the kernel records a timeout and carries on with a zero prefix.
+#include <algorithm>
+
+#include "dvg_device.cuh"
+#include "dvg_internal.h"
+
+namespace dvg {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kTileRows = 32;
+constexpr int kAMax = 512;       // A ranges staged per tile
+constexpr int kSpanMax = 512;    // B rows staged per tile
+constexpr int kBMax = 1536;      // B ranges staged per tile
+constexpr int kBitWords = 10240; // union bitmaps (PRE, SUF, BU) or direct windows
+constexpr int kStageMax = 1536;  // output entries staged per tile
+constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
+constexpr uint32_t kNoStage = 0xffffffffu;
+constexpr unsigned long long kFlag = 1ull << 63;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+enum TileMode : int { kTiled = 0, kDirect = 1, kEmpty = 2 };
+
+struct TileDesc {
+  unsigned long long agg;       // kFlag | entries of the tile
+  unsigned long long agg_nnz;
+  unsigned long long incl;      // kFlag | entries of tiles 0..t
+  unsigned long long incl_nnz;
+};
+
+struct FusedArgs {
+  const uint64_t* __restrict__ a_rowmap;
+  const uint32_t* __restrict__ a_entries;
+  const uint64_t* __restrict__ b_rowmap;
+  const uint32_t* __restrict__ b_entries;
+  uint64_t* __restrict__ c_rowmap;
+  uint32_t* __restrict__ c_entries;
+  uint64_t cap;
+  TileDesc* desc;
+  unsigned* ticket;
+  DeviceControl* ctl;
+  uint32_t nrows;
+  uint32_t ntiles;
+};
+
+struct Smem {
+  uint64_t arow[kTileRows + 1];
+  uint64_t brow[kSpanMax + 1];
+  uint2 a[kAMax];
+  uint2 b[kBMax];
+  uint32_t bits[kBitWords];
+  uint32_t stage[kStageMax];
+  uint32_t rcnt[kTileRows];
+  uint32_t roff[kTileRows];
+  uint32_t rpre[kTileRows];
+  unsigned long long red[kWarps];
+  uint32_t redu[2 * kWarps];
+  unsigned long long prefix;
+  unsigned long long tile_nnz;
+  uint32_t tile;
+  uint32_t stage_used;
+};
+
+// ---- small helpers -----------------------------------------------------------
+
+// Bits of the 32-column word starting at column c0 covered by [rs, re].
+__device__ __forceinline__ uint32_t word_mask(uint32_t rs, uint32_t re, uint64_t c0) {
+  uint64_t lo = max(uint64_t(rs), c0), hi = min(uint64_t(re), c0 + 31);
+  if (rs > re || lo > hi) return 0u;
+  return (~0u << uint32_t(lo - c0)) & (~0u >> uint32_t(31 - (hi - c0)));
+}
+
+// Union of staged B row j on the word starting at c0.
+__device__ __forceinline__ uint32_t row_mask(const Smem& S, uint64_t b_base, uint32_t j, uint64_t c0) {
+  uint32_t k0 = uint32_t((S.brow[j] - b_base) >> 1), k1 = uint32_t((S.brow[j + 1] - b_base) >> 1);
+  uint32_t m = 0;
+  for (uint32_t k = k0; k < k1; ++k) m |= word_mask(S.b[k].x, S.b[k].y, c0);
+  return m;
+}
+
+__device__ __forceinline__ unsigned runtime_group_mask(int g) {
+  return g == 32 ? kFullMask : (((1u << g) - 1u) << (lane_id() & ~(g - 1)));
+}
+
+// Block-wide min and max of a uint32 pair (all threads receive both).
+__device__ void block_minmax(Smem& S, uint32_t& mn, uint32_t& mx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(kFullMask, mn, o));
+    mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
+  }
+  const int w = threadIdx.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    S.redu[w] = mn;
+    S.redu[kWarps + w] = mx;
+  }
+  __syncthreads();
+  mn = S.redu[0];
+  mx = S.redu[kWarps];
+#pragma unroll
+  for (int i = 1; i < kWarps; ++i) {
+    mn = min(mn, S.redu[i]);
+    mx = max(mx, S.redu[kWarps + i]);
+  }
+  __syncthreads();
+}
+
+__device__ unsigned long long block_sum(Smem& S, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) S.red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  unsigned long long s = 0;
+#pragma unroll
+  for (int i = 0; i < kWarps; ++i) s += S.red[i];
+  __syncthreads();
+  return s;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// ---- tiled path: one C row by a group of g lanes over the tile window ------
+
+struct TileGeom {
+  uint64_t a_base, b_base;
+  uint32_t bs;    // first staged B row
+  uint32_t span;  // staged B rows
+  uint64_t base;  // first column of the window (32-aligned)
+  uint32_t nwt;   // window words (the last one is always zero)
+  uint32_t sb;    // union block rows (power of two)
+  uint32_t sb_shift;
+};
+
+// OR of the union bitmaps covering A row r on window word w.
+__device__ __forceinline__ uint32_t tiled_acc(const Smem& S, const TileGeom& T, uint32_t r, uint32_t w) {
+  const uint32_t* PRE = S.bits;
+  const uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
+  const uint32_t* BU = SUF + size_t(T.span) * T.nwt;
+  const uint64_t c0 = T.base + 32ull * w;
+  const uint32_t k0 = uint32_t((S.arow[r] - T.a_base) >> 1), k1 = uint32_t((S.arow[r + 1] - T.a_base) >> 1);
+  uint32_t acc = 0;
+  for (uint32_t k = k0; k < k1; ++k) {
+    const uint2 ar = S.a[k];
+    if (ar.y < ar.x) continue;
+    const uint32_t s = ar.x - T.bs, f = ar.y - T.bs;
+    const uint32_t bS = s >> T.sb_shift, bF = f >> T.sb_shift;
+    if (bS == bF) {
+      for (uint32_t j = s; j <= f; ++j) acc |= row_mask(S, T.b_base, j, c0);
+    } else {
+      acc |= SUF[size_t(s) * T.nwt + w] | PRE[size_t(f) * T.nwt + w];
+      for (uint32_t bb = bS + 1; bb < bF; ++bb) acc |= BU[size_t(bb) * T.nwt + w];
+    }
+  }
+  return acc;
+}
+
+// Gathers the runs of one window chunk held by the group (word w per lane).
+// Emits through `emit(row_local_index, value)`; returns the chunk's boundary
+// count (group-uniform) and updates `carry` (msb of the chunk's last word).
+template <class Emit>
+__device__ __forceinline__ uint32_t gather_chunk(uint32_t x, bool valid, uint64_t c0, int g, int lg, unsigned gm,
+                                                 uint32_t& carry, uint64_t count, uint32_t last_lane, Emit&& emit) {
+  uint32_t prev = __shfl_up_sync(gm, x, 1, g);
+  uint32_t c = lg == 0 ? carry : (prev >> 31);
+  uint32_t sh = (x << 1) | c;
+  uint32_t bnd = valid ? (((x ^ sh) & x) | (sh & ~x)) : 0u;
+  uint32_t cnt = __popc(bnd);
+  uint32_t incl = cnt;
+  for (int o = 1; o < g; o <<= 1) {
+    uint32_t u = __shfl_up_sync(gm, incl, o, g);
+    if (lg >= o) incl += u;
+  }
+  uint64_t k = count + incl - cnt;
+  while (bnd) {
+    int bit = __ffs(bnd) - 1;
+    bnd &= bnd - 1;
+    emit(k, uint32_t(c0 + bit - (k & 1)));
+    ++k;
+  }
+  uint32_t total = __shfl_sync(gm, incl, g - 1, g);
+  carry = __shfl_sync(gm, x, int(last_lane), g) >> 31;
+  return total;
+}
+
+// Processes C row r of a tiled tile.  count_only: returns the entry count and
+// adds the row's nnz into nnz_acc (per lane).  Otherwise emits through `emit`.
+template <class Emit>
+__device__ uint32_t tiled_row(const Smem& S, const TileGeom& T, uint32_t r, int g, int lg, unsigned gm,
+                              unsigned long long* nnz_acc, Emit&& emit) {
+  uint32_t carry = 0;
+  uint64_t count = 0;
+  for (uint32_t wb = 0; wb < T.nwt; wb += g) {
+    const uint32_t w = wb + lg;
+    const bool valid = w < T.nwt;
+    const uint32_t x = valid ? tiled_acc(S, T, r, w) : 0u;
+    if (nnz_acc) *nnz_acc += __popc(x);
+    const uint32_t last = min(uint32_t(g - 1), T.nwt - 1 - wb);
+    count += gather_chunk(x, valid, T.base + 32ull * w, g, lg, gm, carry, count, last, emit);
+  }
+  return uint32_t(count);
+}
+
+// ---- direct path: one C row by a warp, bitvector window in shared memory ----
+
+template <class Emit>
+__device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row, uint32_t* bits, uint32_t* reach,
+                               unsigned long long* nnz_acc, Emit&& emit) {
+  const int lg = lane_id();
+  uint64_t a0, a1;
+  if (a_identity) {
+    a0 = 0;
+    a1 = 2;
+  } else {
+    a0 = p.a_rowmap[row];
+    a1 = p.a_rowmap[row + 1];
+  }
+  auto slice = [&](uint64_t ai, uint64_t& b0, uint64_t& b1) {
+    uint32_t s, f;
+    if (a_identity) {
+      s = f = uint32_t(row);
+    } else {
+      uint2 r = load_range(p.a_entries, ai >> 1);
+      s = r.x;
+      f = r.y;
+    }
+    if (f < s) {
+      b0 = b1 = 0;
+      return;
+    }
+    b0 = p.b_rowmap[s] >> 1;
+    b1 = p.b_rowmap[uint64_t(f) + 1] >> 1;
+  };
+  uint32_t mn = 0xffffffffu, mx = 0;
+  for (uint64_t ai = a0; ai < a1; ai += 2) {
+    uint64_t b0, b1;
+    slice(ai, b0, b1);
+    for (uint64_t t = b0 + lg; t < b1; t += 32) {
+      uint2 r = load_range(p.b_entries, t);
+      if (r.y < r.x) continue;
+      mn = min(mn, r.x);
+      mx = max(mx, r.y);
+    }
+  }
+  mn = group_min<32>(kFullMask, mn);
+  mx = group_max<32>(kFullMask, mx);
+  uint64_t count = 0;
+  if (mn > mx) return 0;
+  const uint64_t base = mn & ~31u;
+  const uint64_t nw_total = ((uint64_t(mx) - base) >> 5) + 2;
+  uint32_t carry = 0;
+  for (uint64_t w0 = 0; w0 < nw_total; w0 += kDirectWW) {
+    const uint32_t nwc = uint32_t(min(uint64_t(kDirectWW), nw_total - w0));
+    const uint64_t cb = base + 32 * w0;
+    const uint64_t ce = cb + 32ull * nwc - 1;
+    for (uint32_t w = lg; w < nwc; w += 32) {
+      bits[w] = 0;
+      reach[w] = 0;
+    }
+    __syncwarp();
+    for (uint64_t ai = a0; ai < a1; ai += 2) {
+      uint64_t b0, b1;
+      slice(ai, b0, b1);
+      for (uint64_t t = b0 + lg; t < b1; t += 32) {
+        uint2 r = load_range(p.b_entries, t);
+        uint64_t cs = max(uint64_t(r.x), cb);
+        uint64_t cf = min(uint64_t(r.y), ce);
+        if (cs > cf || r.y < r.x) continue;
+        uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
+        uint32_t lo = ~0u << (cs & 31);
+        uint32_t hi = ~0u >> (31 - (cf & 31));
+        if (ws == we) {
+          atomicOr(bits + ws, lo & hi);
+        } else {
+          atomicOr(bits + ws, lo);
+          atomicOr(bits + we, hi);
+          if (we > ws + 1) atomicMax(reach + ws + 1, we);
+        }
+      }
+    }
+    __syncwarp();
+    uint32_t run_reach = 0;
+    for (uint32_t wb = 0; wb < nwc; wb += 32) {
+      const uint32_t w = wb + lg;
+      const bool valid = w < nwc;
+      uint32_t x = 0, rr = 0;
+      if (valid) {
+        x = bits[w];
+        rr = reach[w];
+      }
+      rr = group_incl_max<32>(kFullMask, rr, lg);
+      rr = max(rr, run_reach);
+      if (valid && rr > w) x = ~0u;
+      run_reach = __shfl_sync(kFullMask, rr, 31);
+      if (nnz_acc) *nnz_acc += __popc(x);
+      const uint32_t last = min(31u, nwc - 1 - wb);
+      count += gather_chunk(x, valid, cb + 32ull * w, 32, lg, kFullMask, carry, count, last, emit);
+    }
+    __syncwarp();
+  }
+  return count;
+}
+
+// ---- decoupled look-back over the tile ticket order -------------------------
+
+__device__ void lookback(const FusedArgs& p, uint32_t t, unsigned long long cnt, unsigned long long nnz,
+                         unsigned long long& prefix, unsigned long long& prefix_nnz) {
+  TileDesc* d = p.desc;
+  if (t == 0) {
+    prefix = 0;
+    prefix_nnz = 0;
+    d[0].incl_nnz = nnz;
+    st_release(&d[0].incl, kFlag | cnt);
+    return;
+  }
+  d[t].agg_nnz = nnz;
+  st_release(&d[t].agg, kFlag | cnt);
+  unsigned long long pre = 0, pre_nnz = 0;
+  int64_t j = int64_t(t) - 1;
+  uint32_t spins = 0;
+  bool timed_out = false;
+  while (j >= 0) {
+    unsigned long long v = ld_acquire(&d[j].incl);
+    if (v & kFlag) {
+      pre += v & ~kFlag;
+      pre_nnz += *reinterpret_cast<volatile unsigned long long*>(&d[j].incl_nnz);
+      break;
+    }
+    v = ld_acquire(&d[j].agg);
+    if (v & kFlag) {
+      pre += v & ~kFlag;
+      pre_nnz += *reinterpret_cast<volatile unsigned long long*>(&d[j].agg_nnz);
+      --j;
+      continue;
+    }
+    if (++spins > kSpinLimit) {
+      timed_out = true;
+      break;
+    }
+    __nanosleep(64);
+  }
+  if (timed_out) atomicOr(&p.ctl->timeout, 1ull);
+  prefix = pre;
+  prefix_nnz = pre_nnz;
+  d[t].incl_nnz = pre_nnz + nnz;
+  st_release(&d[t].incl, kFlag | (pre + cnt));
+}
+
+template <bool A_ID>
+__global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  while (true) {
+    if (tid == 0) S.tile = atomicAdd(p.ticket, 1u);
+    __syncthreads();
+    const uint32_t t = S.tile;
+    if (t >= p.ntiles) break;
+    const uint32_t i0 = t * kTileRows;
+    const uint32_t rows = min(uint32_t(kTileRows), p.nrows - i0);
+    int mode = kTiled;
+    TileGeom T{};
+    unsigned long long nnz_acc = 0;
+
+    // 1. A tile
+    uint64_t a_cnt;
+    if (A_ID) {
+      if (tid <= int(rows)) S.arow[tid] = 2ull * tid;
+      if (tid < int(rows)) S.a[tid] = make_uint2(i0 + tid, i0 + tid);
+      T.a_base = 0;
+      a_cnt = rows;
+    } else {
+      if (tid <= int(rows)) S.arow[tid] = p.a_rowmap[i0 + tid];
+      __syncthreads();
+      T.a_base = S.arow[0];
+      a_cnt = (S.arow[rows] - T.a_base) >> 1;
+      if (a_cnt > kAMax) {
+        mode = kDirect;
+      } else {
+        for (uint32_t k = tid; k < a_cnt; k += kThreads) S.a[k] = load_range(p.a_entries, (T.a_base >> 1) + k);
+      }
+    }
+    if (tid == 0) S.stage_used = 0;
+    __syncthreads();
+
+    // 2. B rows named by the tile
+    if (mode == kTiled) {
+      uint32_t mn = 0xffffffffu, mx = 0;
+      for (uint32_t k = tid; k < a_cnt; k += kThreads) {
+        uint2 r = S.a[k];
+        if (r.y >= r.x) {
+          mn = min(mn, r.x);
+          mx = max(mx, r.y);
+        }
+      }
+      block_minmax(S, mn, mx);
+      if (mn > mx) {
+        mode = kEmpty;
+      } else {
+        T.bs = mn;
+        T.span = mx - mn + 1;
+        if (T.span > kSpanMax) mode = kDirect;
+      }
+    }
+    if (mode == kTiled) {
+      for (uint32_t k = tid; k <= T.span; k += kThreads) S.brow[k] = p.b_rowmap[uint64_t(T.bs) + k];
+      __syncthreads();
+      T.b_base = S.brow[0];
+      const uint64_t b_cnt = (S.brow[T.span] - T.b_base) >> 1;
+      if (b_cnt > kBMax) {
+        mode = kDirect;
+      } else {
+        for (uint32_t k = tid; k < b_cnt; k += kThreads) S.b[k] = load_range(p.b_entries, (T.b_base >> 1) + k);
+      }
+      __syncthreads();
+      if (mode == kTiled) {
+        uint32_t mn = 0xffffffffu, mx = 0;
+        for (uint32_t k = tid; k < b_cnt; k += kThreads) {
+          uint2 r = S.b[k];
+          if (r.y >= r.x) {
+            mn = min(mn, r.x);
+            mx = max(mx, r.y);
+          }
+        }
+        uint32_t wmax = 0;  // widest A range (rows)
+        for (uint32_t k = tid; k < a_cnt; k += kThreads) {
+          uint2 r = S.a[k];
+          if (r.y >= r.x) wmax = max(wmax, r.y - r.x + 1);
+        }
+        block_minmax(S, mn, mx);
+        uint32_t zero = 0;
+        block_minmax(S, zero, wmax);
+        if (mn > mx) {
+          mode = kEmpty;
+        } else {
+          T.base = mn & ~31u;
+          T.nwt = uint32_t(((uint64_t(mx) - T.base) >> 5) + 2);
+          // union block: about half the widest A range, 2..64 rows
+          uint32_t sb = 2;
+          while (sb < 64 && sb * 4 <= wmax) sb <<= 1;
+          T.sb = sb;
+          T.sb_shift = __ffs(sb) - 1;
+          const uint64_t nblk = (T.span + sb - 1) >> T.sb_shift;
+          const uint64_t need = (2ull * T.span + nblk) * T.nwt;
+          if (need > kBitWords) mode = kDirect;
+        }
+      }
+    }
+
+    // 3. union bitmaps: R_j into PRE, then SUF (from R) and PRE (in place)
+    if (mode == kTiled) {
+      uint32_t* PRE = S.bits;
+      uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
+      uint32_t* BU = SUF + size_t(T.span) * T.nwt;
+      const uint32_t items = T.span * T.nwt;
+      for (uint32_t it = tid; it < items; it += kThreads) {
+        const uint32_t j = it / T.nwt, w = it - j * T.nwt;
+        PRE[it] = row_mask(S, T.b_base, j, T.base + 32ull * w);
+      }
+      __syncthreads();
+      const uint32_t nblk = (T.span + T.sb - 1) >> T.sb_shift;
+      for (uint32_t it = tid; it < nblk * T.nwt; it += kThreads) {
+        const uint32_t bb = it / T.nwt, w = it - bb * T.nwt;
+        const uint32_t j0 = bb << T.sb_shift, j1 = min(T.span, j0 + T.sb);
+        uint32_t acc = 0;
+        for (uint32_t j = j1; j-- > j0;) {
+          acc |= PRE[size_t(j) * T.nwt + w];
+          SUF[size_t(j) * T.nwt + w] = acc;
+        }
+        acc = 0;
+        for (uint32_t j = j0; j < j1; ++j) {
+          acc |= PRE[size_t(j) * T.nwt + w];
+          PRE[size_t(j) * T.nwt + w] = acc;
+        }
+        BU[size_t(bb) * T.nwt + w] = acc;
+      }
+      __syncthreads();
+
+      // 4. rows: groups of g lanes, each lane one window word per chunk
+      const int g = T.nwt <= 4 ? 4 : T.nwt <= 8 ? 8 : T.nwt <= 16 ? 16 : 32;
+      const int lg = tid & (g - 1);
+      const unsigned gm = runtime_group_mask(g);
+      for (uint32_t r = tid / g; r < rows; r += kThreads / g) {
+        uint32_t slot = 0;
+        uint32_t cnt = 0;
+        if (T.nwt <= uint32_t(g)) {
+          // one chunk: the row stays in registers between count and write
+          const bool valid = uint32_t(lg) < T.nwt;
+          const uint32_t x = valid ? tiled_acc(S, T, r, lg) : 0u;
+          nnz_acc += __popc(x);
+          uint32_t carry = 0;
+          // count first (emit nothing), then write with the slot known
+          uint32_t c2 = carry;
+          cnt = gather_chunk(x, valid, 0, g, lg, gm, c2, 0, T.nwt - 1, [](uint64_t, uint32_t) {});
+          if (lg == 0) slot = atomicAdd(&S.stage_used, cnt);
+          slot = __shfl_sync(gm, slot, 0, g);
+          const bool fits = slot + cnt <= uint32_t(kStageMax);
+          if (fits) {
+            uint32_t* st = S.stage + slot;
+            c2 = 0;
+            gather_chunk(x, valid, T.base + 32ull * lg, g, lg, gm, c2, 0, T.nwt - 1,
+                         [&](uint64_t k, uint32_t v) { st[k] = v; });
+          }
+          if (lg == 0) {
+            S.rcnt[r] = cnt;
+            S.roff[r] = fits ? slot : kNoStage;
+          }
+        } else {
+          cnt = tiled_row(S, T, r, g, lg, gm, &nnz_acc, [](uint64_t, uint32_t) {});
+          if (lg == 0) slot = atomicAdd(&S.stage_used, cnt);
+          slot = __shfl_sync(gm, slot, 0, g);
+          const bool fits = slot + cnt <= uint32_t(kStageMax);
+          if (fits) {
+            uint32_t* st = S.stage + slot;
+            tiled_row(S, T, r, g, lg, gm, nullptr, [&](uint64_t k, uint32_t v) { st[k] = v; });
+          }
+          if (lg == 0) {
+            S.rcnt[r] = cnt;
+            S.roff[r] = fits ? slot : kNoStage;
+          }
+        }
+      }
+    } else if (mode == kDirect) {
+      uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
+      uint32_t* reach = bits + kDirectWW;
+      for (uint32_t r = warp; r < rows; r += kWarps) {
+        uint64_t c = direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, &nnz_acc, [](uint64_t, uint32_t) {});
+        if (lane == 0) {
+          S.rcnt[r] = uint32_t(c);
+          S.roff[r] = kNoStage;
+        }
+      }
+    } else {
+      if (tid < int(rows)) {
+        S.rcnt[tid] = 0;
+        S.roff[tid] = 0;
+      }
+    }
+    __syncthreads();
+
+    // 5. tile totals and the look-back
+    const unsigned long long tile_nnz = block_sum(S, nnz_acc);
+    if (warp == 0) {
+      uint32_t v = lane < int(rows) ? S.rcnt[lane] : 0u;
+      uint32_t incl = group_incl_sum<32>(kFullMask, v, lane);
+      if (lane < int(rows)) S.rpre[lane] = incl - v;
+      const unsigned long long tile_cnt = __shfl_sync(kFullMask, incl, 31);
+      if (lane == 0) {
+        unsigned long long pre, pre_nnz;
+        lookback(p, t, tile_cnt, tile_nnz, pre, pre_nnz);
+        S.prefix = pre;
+        if (t == p.ntiles - 1) {
+          p.ctl->total = pre + tile_cnt;
+          p.ctl->nnz = pre_nnz + tile_nnz;
+          if (pre + tile_cnt > p.cap) p.ctl->overflow = pre + tile_cnt;
+        }
+        if (mode == kDirect) atomicAdd(&p.ctl->tiles_direct, 1ull);
+      }
+    }
+    __syncthreads();
+    const unsigned long long prefix = S.prefix;
+
+    // 6. rowmap and entries
+    if (tid < int(rows)) p.c_rowmap[uint64_t(i0) + tid + 1] = prefix + S.rpre[tid] + S.rcnt[tid];
+    if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
+    for (uint32_t r = warp; r < rows; r += kWarps) {
+      const uint32_t n = S.rcnt[r];
+      const unsigned long long dst = prefix + S.rpre[r];
+      if (n == 0) continue;
+      if (dst + n > p.cap) {
+        if (lane == 0) atomicOr(&p.ctl->overflow, 1ull);
+        continue;
+      }
+      if (S.roff[r] != kNoStage) {
+        const uint32_t* src = S.stage + S.roff[r];
+        for (uint32_t k = lane; k < n; k += 32) p.c_entries[dst + k] = src[k];
+      } else if (mode == kDirect) {
+        uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
+        uint32_t* reach = bits + kDirectWW;
+        uint32_t* out = p.c_entries + dst;
+        bool bad = false;
+        uint64_t c = direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
+          if (k < n) out[k] = v;
+          else bad = true;
+        });
+        if (bad || c != n) atomicOr(&p.ctl->status, 8ull);
+      }
+    }
+    if (mode == kTiled) {
+      // rows that did not fit the staging buffer: recompute into global memory
+      const int g = T.nwt <= 4 ? 4 : T.nwt <= 8 ? 8 : T.nwt <= 16 ? 16 : 32;
+      const int lg = tid & (g - 1);
+      const unsigned gm = runtime_group_mask(g);
+      for (uint32_t r = tid / g; r < rows; r += kThreads / g) {
+        if (S.roff[r] != kNoStage || S.rcnt[r] == 0) continue;
+        const uint32_t n = S.rcnt[r];
+        const unsigned long long dst = prefix + S.rpre[r];
+        if (dst + n > p.cap) continue;
+        uint32_t* out = p.c_entries + dst;
+        tiled_row(S, T, r, g, lg, gm, nullptr, [&](uint64_t k, uint32_t v) {
+          if (k < n) out[k] = v;
+        });
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
+                         uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
+  const uint32_t n = a_identity ? b->nrows : a->nrows;
+  if (n == 0) return;
+  const uint32_t ntiles = (n + kTileRows - 1) / kTileRows;
+  const size_t desc_bytes = size_t(ntiles) * sizeof(TileDesc);
+  if (desc_bytes > ctx->tile_desc_cap) {
+    if (ctx->d_tile_desc) dfree(ctx, ctx->d_tile_desc);
+    ctx->d_tile_desc = nullptr;
+    ctx->tile_desc_cap = 0;
+    size_t want = std::max(desc_bytes, size_t(1) << 20);
+    ctx->d_tile_desc = dalloc(ctx, want);
+    ctx->tile_desc_cap = want;
+  }
+  if (!ctx->d_ticket) ctx->d_ticket = static_cast<unsigned*>(dalloc(ctx, 256));
+  DVG_CUDA(cudaMemsetAsync(ctx->d_tile_desc, 0, desc_bytes, ctx->stream));
+  DVG_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(unsigned), ctx->stream));
+  FusedArgs p{};
+  p.a_rowmap = a_identity ? nullptr : a->rowmap;
+  p.a_entries = a_identity ? nullptr : a->entries;
+  p.b_rowmap = b->rowmap;
+  p.b_entries = b->entries;
+  p.c_rowmap = c_rowmap;
+  p.c_entries = c_entries;
+  p.cap = cap;
+  p.desc = static_cast<TileDesc*>(ctx->d_tile_desc);
+  p.ticket = ctx->d_ticket;
+  p.ctl = ctx->d_ctl;
+  p.nrows = n;
+  p.ntiles = ntiles;
+  auto kern = a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>;
+  const int smem = int(sizeof(Smem));
+  DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+  if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "fused spgemm: shared memory layout does not fit");
+  const unsigned grid = unsigned(std::min<uint64_t>(ntiles, uint64_t(per_sm) * ctx->num_sms));
+  kern<<<grid, kThreads, smem, ctx->stream>>>(p);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+}  // namespace dvg

@@ -61,6 +61,8 @@ typedef struct dvg_stats {
   uint64_t spgemm_numeric_ns;   /* SpGEMM numeric passes */
   uint64_t scan_ns;             /* rowmap scans (SpGEMM and SpAdd) */
   uint64_t spadd_ns;            /* SpAdd passes */
+  uint64_t spgemm_direct_tiles; /* SpGEMM row tiles that missed the staged path */
+  uint64_t spgemm_reruns;       /* SpGEMMs re-run after an output capacity overflow */
 } dvg_stats;
 
 /* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /
@@ -76,9 +78,11 @@ dvg_status dvg_shutdown(dvg_context* ctx);
  * context's own stream). */
 dvg_status dvg_set_stream(dvg_context* ctx, void* cuda_stream);
 dvg_status dvg_synchronize(dvg_context* ctx);
-/* Tuning knobs: "group_lanes" (0 = autotune, or 4/8/16/32 lanes per output
- * row), "window_words" (0 = default, else 32-bit words of accumulator per row
- * group), "timing" (1 = time kernels with CUDA events into dvg_stats). */
+/* Tuning knobs: "algo" (0 = fused single-pass tile-staged SpGEMM, the
+ * default; 1 = two-pass row-direct SpGEMM), "group_lanes" (two-pass path: 0 =
+ * autotune, or 4/8/16/32 lanes per output row), "window_words" (two-pass path:
+ * 0 = default, else 32-bit accumulator words per row group), "timing" (1 =
+ * time kernels with CUDA events into dvg_stats). */
 dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value);
 dvg_status dvg_get_stats(const dvg_context* ctx, dvg_stats* out);
 dvg_status dvg_stats_reset(dvg_context* ctx);

@@ -10,9 +10,11 @@ from tests.conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-# group sizes x accumulator windows: "auto", every group size at its default
-# window, and tiny windows that force the multi-chunk path
-PLANS = [(0, 0), (4, 0), (8, 0), (16, 0), (32, 0), (4, 1), (8, 3), (32, 2), (16, 37)]
+# (algo, group lanes, window words): the fused tile-staged kernel, then the
+# two-pass row-direct kernel at "auto", every group size at its default
+# window, and tiny windows that force its multi-chunk path
+PLANS = [(0, 0, 0), (1, 0, 0), (1, 4, 0), (1, 8, 0), (1, 16, 0), (1, 32, 0), (1, 4, 1), (1, 8, 3), (1, 32, 2),
+         (1, 16, 37)]
 
 
 @pytest.fixture(scope="module")
@@ -23,8 +25,9 @@ def ctx():
 
 
 def set_plan(ctx, plan):
-    ctx.set_option("group_lanes", plan[0])
-    ctx.set_option("window_words", plan[1])
+    ctx.set_option("algo", plan[0])
+    ctx.set_option("group_lanes", plan[1])
+    ctx.set_option("window_words", plan[2])
 
 
 def as_crs(o):
@@ -54,7 +57,7 @@ def test_hbitvector_known_answer(ctx, plan):
 
 
 @pytest.mark.parametrize("name", ["x", "multi", "m"])
-@pytest.mark.parametrize("plan", [(0, 0), (4, 0), (32, 0), (8, 3)])
+@pytest.mark.parametrize("plan", [(0, 0, 0), (1, 0, 0), (1, 4, 0), (1, 32, 0), (1, 8, 3)])
 def test_gfa_fixture_products(ctx, name, plan):
     set_plan(ctx, plan)
     g = load_golden(f"gfa_{name}.npz")
@@ -84,7 +87,7 @@ def test_random_spgemm_reference_shape(ctx, plan):
     assert_same(ctx.spgemm(da, da).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", [(0, 0), (4, 0), (16, 0), (8, 5)])
+@pytest.mark.parametrize("plan", [(0, 0, 0), (1, 0, 0), (1, 4, 0), (1, 16, 0), (1, 8, 5)])
 def test_random_power_reference_shape(ctx, plan):
     # test_range_sparse.cpp:590-594: N = 6521, NNZ = 4000, K = 100
     set_plan(ctx, plan)
@@ -102,8 +105,9 @@ def test_random_spadd_reference_shapes(ctx, n, nnz):
     assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
 
 
-def test_rectangular_spgemm(ctx):
-    set_plan(ctx, (0, 0))
+@pytest.mark.parametrize("algo", [0, 1])
+def test_rectangular_spgemm(ctx, algo):
+    set_plan(ctx, (algo, 0, 0))
     a = gen.random_matrix(3000, 30000, seed=5)
     b = gen.banded(3000, 64, 3.0, 16.0, seed=6)
     # a: 3000 x 3000, b: 3000 x 3000 -> check A*B and B*A
@@ -112,7 +116,7 @@ def test_rectangular_spgemm(ctx):
         assert_same(ctx.spgemm(ctx.upload(x), ctx.upload(y)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", [(0, 0), (8, 0), (32, 4)])
+@pytest.mark.parametrize("plan", [(0, 0, 0), (1, 0, 0), (1, 8, 0), (1, 32, 4)])
 def test_banded_spgemm(ctx, plan):
     set_plan(ctx, plan)
     a = gen.banded(1 << 16, 512, 4.0, 32.0, seed=31)
@@ -123,23 +127,75 @@ def test_banded_spgemm(ctx, plan):
     assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
 
 
+@pytest.mark.parametrize("algo", [0, 1])
 @pytest.mark.parametrize("window", [(100, 300), (0, 250), (150, 450), (1, 1), (7, 7), (0, 1)])
-def test_small_graph_index(ctx, window):
-    set_plan(ctx, (0, 0))
+def test_small_graph_index(ctx, window, algo):
+    set_plan(ctx, (algo, 0, 0))
     a, _ = gen.graph_adjacency(gen.small_graph_spec(100_000, seed=42))
     want = orc.dindex(omat(a), window[0], window[1], algo="hbv")
     got = ctx.distance_index(ctx.upload(a), *window).download()
     assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
 
 
-def test_graph_with_structural_bubbles_index(ctx):
-    set_plan(ctx, (0, 0))
+@pytest.mark.parametrize("algo", [0, 1])
+def test_graph_with_structural_bubbles_index(ctx, algo):
+    set_plan(ctx, (algo, 0, 0))
     spec = gen.GraphSpec(60_000, 1e-3, 2e-4, 0.5, 1, 50, 4.0, 0.05, 100, 2000, seed=8)
     a, st = gen.graph_adjacency(spec)
     assert st["n_sv"] > 0
     want = orc.dindex(omat(a), 400, 600, algo="hbv")
     got = ctx.distance_index(ctx.upload(a), 400, 600).download()
     assert_same(got, want.rowmap, want.entries, want.nnz)
+
+
+def spgemm_case(ctx, a, b, expect_direct=None):
+    want = orc.spgemm(omat(a), omat(b), algo="hbv")
+    ctx.reset_stats()
+    got = ctx.spgemm(ctx.upload(a), ctx.upload(b)).download()
+    assert_same(got, want.rowmap, want.entries, want.nnz)
+    return ctx.stats()
+
+
+def test_fused_tiled_single_chunk_and_stage_overflow(ctx):
+    # narrow band, many short output runs: staged tiles whose output exceeds
+    # the staging buffer and is recomputed into global memory
+    set_plan(ctx, (0, 0, 0))
+    a = gen.banded(20_000, 20, 3.0, 1.0, seed=41)
+    b = gen.banded(20_000, 300, 10.0, 1.0, seed=42)
+    st = spgemm_case(ctx, a, b)
+    assert st["spgemm_direct_tiles"] == 0
+
+
+def test_fused_tiled_multi_chunk(ctx):
+    # a tile window wider than 32 words: lane groups loop over window chunks
+    set_plan(ctx, (0, 0, 0))
+    a = gen.banded(20_000, 20, 3.0, 1.0, seed=43)
+    b = gen.banded(20_000, 600, 10.0, 1.0, seed=44)
+    st = spgemm_case(ctx, a, b)
+    assert st["spgemm_direct_tiles"] == 0
+
+
+def test_fused_direct_tiles_and_capacity_rerun(ctx):
+    # random columns: every tile misses the staged path; the output exceeds the
+    # speculative capacity, which is detected and re-run at the exact size
+    set_plan(ctx, (0, 0, 0))
+    a = gen.random_matrix(2000, 8000, seed=45)
+    b = gen.random_matrix(2000, 30000, seed=46)
+    st = spgemm_case(ctx, a, b)
+    assert st["spgemm_direct_tiles"] > 0
+    assert st["spgemm_reruns"] == 1
+
+
+def test_algos_agree_on_cfg2_shape_sample(ctx):
+    # the kernel microbenchmark shape (banded, half-width 512, Poisson(4)
+    # ranges of geometric length 32) at 2^20 rows: both kernels and the oracle
+    a = gen.banded(1 << 20, 512, 4.0, 32.0, seed=51)
+    b = gen.banded(1 << 20, 512, 4.0, 32.0, seed=52)
+    want = orc.spgemm(omat(a), omat(b), algo="hbv")
+    for algo in (0, 1):
+        set_plan(ctx, (algo, 0, 0))
+        got = ctx.spgemm(ctx.upload(a), ctx.upload(b)).download()
+        assert_same(got, want.rowmap, want.entries, want.nnz, f"algo {algo}")
 
 
 def test_query_batch_matches_oracle(ctx):
