@@ -462,6 +462,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "algo")) {
       require(value == 0 || value == 1, "algo must be 0 (fused tiled) or 1 (two-pass direct)");
       ctx->opt_algo = value;
+    } else if (!std::strcmp(key, "chunk_rows")) {
+      require(value >= 0 && value <= 2048 && value % 32 == 0, "chunk_rows must be 0 or a multiple of 32 up to 2048");
+      ctx->opt_chunk_rows = value;
     } else if (!std::strcmp(key, "timing")) {
       DVG_CUDA(cudaStreamSynchronize(ctx->stream));
       resolve_spans(ctx);

@@ -55,6 +55,7 @@ struct dvg_context {
   int64_t opt_group_lanes = 0;
   int64_t opt_window_words = 0;
   int64_t opt_algo = 0;               // 0: fused tiled SpGEMM, 1: two-pass direct
+  int64_t opt_chunk_rows = 0;         // fused SpGEMM look-back chunk rows (0: automatic)
   bool opt_timing = false;
   // event pairs bracketing timed kernels, resolved at the next stream sync
   struct TimedSpan {

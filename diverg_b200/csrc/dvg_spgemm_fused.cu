@@ -6,29 +6,31 @@
 // row r of C is the union of all ranges of B rows s..f for every range
 // [s,f] of A's row r, emitted as sorted maximal runs.
 //
-// The kernel is persistent: each CTA takes tiles of kTileRows consecutive C
-// rows from an atomic ticket, so tiles start in order, and
-//  1. stages the tile's A ranges and the slice of B rows they name (one
+// The kernel is persistent.  Each CTA takes chunks of consecutive C rows from
+// an atomic ticket (so chunks start in order) and walks a chunk in sub-tiles
+// of kSubRows rows.  For every sub-tile it
+//  1. stages the sub-tile's A ranges and the slice of B rows they name (one
 //     contiguous rowmap window and one contiguous entries window) in shared
 //     memory;
-//  2. builds, over the staged B rows, union bitmaps on the tile's column
-//     window: for blocks of `sb` rows, the prefix union PRE[j] (block start
-//     .. j), the suffix union SUF[j] (j .. block end) and the block union
-//     BU[b].  A range [s,f] of A then costs SUF[s] | BU[..] | PRE[f] -- a few
-//     word ORs per column word -- instead of one visit per B row, which is
-//     what dominates products of wide-range matrices (powers of A+I);
+//  2. builds, over the staged B rows, union bitmaps on the sub-tile's column
+//     window: for blocks of `sb` rows the prefix union PRE[j] (block start ..
+//     j), the suffix union SUF[j] (j .. block end) and the block union BU[b].
+//     A range [s,f] of A then costs SUF[s] | BU[..] | PRE[f] -- a few word
+//     ORs per column word -- instead of one visit per B row, which is what
+//     dominates products of wide-range matrices (powers of A+I);
 //  3. gathers every C row from those words with the boundary masks of the
 //     reference's HBitVector gather (map01 / map10, hbitvector.hpp:568-597):
 //     popc counts, a lane-group prefix sum places, ffs extracts;
-//  4. stages the row runs in shared memory, obtains the tile's output offset
-//     by decoupled look-back over the tile ticket order (no separate
-//     symbolic pass or scan kernel), then writes c_rowmap and c_entries
-//     with coalesced stores.
-// Tiles whose A ranges, B slice or column window exceed the staging buffers
-// take the direct path: a warp per row accumulates the B ranges in a shared
-// bitvector window (column chunks when the band is wider), counts, joins the
-// look-back, then recomputes and writes.  Look-back waits are bounded; on
-// expiry the kernel records a timeout and carries on with a zero prefix.
+//  4. appends the rows' runs, in row order, to a shared-memory staging area.
+// At the end of the chunk a warp-parallel decoupled look-back over the chunk
+// order yields the chunk's output offset (no separate symbolic pass or scan
+// kernel); c_rowmap and the staged entries are then written with coalesced
+// stores.  Sub-tiles whose A ranges, B slice or column window exceed the
+// staging buffers take the direct path (a warp per row accumulates the B
+// ranges in a shared bitvector window, in column chunks when the band is
+// wider); rows that no longer fit the staging area are recomputed by the
+// direct path straight into global memory after the look-back.  Look-back
+// waits are bounded: on expiry the kernel records a timeout.
 #include <algorithm>
 
 #include "dvg_device.cuh"
@@ -39,23 +41,23 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kTileRows = 32;
-constexpr int kAMax = 512;       // A ranges staged per tile
-constexpr int kSpanMax = 512;    // B rows staged per tile
-constexpr int kBMax = 1536;      // B ranges staged per tile
-constexpr int kBitWords = 10240; // union bitmaps (PRE, SUF, BU) or direct windows
-constexpr int kStageMax = 1536;  // output entries staged per tile
+constexpr int kSubRows = 32;      // rows per staged sub-tile
+constexpr int kChunkMax = 2048;   // rows per look-back chunk (upper bound)
+constexpr int kAMax = 256;        // A ranges staged per sub-tile
+constexpr int kSpanMax = 512;     // B rows staged per sub-tile
+constexpr int kBMax = 1024;       // B ranges staged per sub-tile
+constexpr int kBitWords = 7168;   // union bitmaps (PRE, SUF, BU) or direct windows
+constexpr int kStageMax = 6144;   // output entries staged per chunk
 constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
-constexpr uint32_t kNoStage = 0xffffffffu;
 constexpr unsigned long long kFlag = 1ull << 63;
 constexpr uint32_t kSpinLimit = 1u << 22;
 
 enum TileMode : int { kTiled = 0, kDirect = 1, kEmpty = 2 };
 
-struct TileDesc {
-  unsigned long long agg;       // kFlag | entries of the tile
+struct ChunkDesc {
+  unsigned long long agg;       // kFlag | entries of the chunk
   unsigned long long agg_nnz;
-  unsigned long long incl;      // kFlag | entries of tiles 0..t
+  unsigned long long incl;      // kFlag | entries of chunks 0..t
   unsigned long long incl_nnz;
 };
 
@@ -67,29 +69,31 @@ struct FusedArgs {
   uint64_t* __restrict__ c_rowmap;
   uint32_t* __restrict__ c_entries;
   uint64_t cap;
-  TileDesc* desc;
+  ChunkDesc* desc;
   unsigned* ticket;
   DeviceControl* ctl;
   uint32_t nrows;
-  uint32_t ntiles;
+  uint32_t chunk_rows;  // multiple of kSubRows, <= kChunkMax
+  uint32_t nchunks;
 };
 
 struct Smem {
-  uint64_t arow[kTileRows + 1];
+  uint64_t arow[kSubRows + 1];
   uint64_t brow[kSpanMax + 1];
   uint2 a[kAMax];
   uint2 b[kBMax];
   uint32_t bits[kBitWords];
   uint32_t stage[kStageMax];
-  uint32_t rcnt[kTileRows];
-  uint32_t roff[kTileRows];
-  uint32_t rpre[kTileRows];
+  uint32_t incl[kChunkMax];       // row entry counts, then their inclusive prefix
+  uint32_t sub_off[kSubRows];     // stage offset of each row of the sub-tile
   unsigned long long red[kWarps];
   uint32_t redu[2 * kWarps];
   unsigned long long prefix;
-  unsigned long long tile_nnz;
-  uint32_t tile;
-  uint32_t stage_used;
+  uint32_t chunk;
+  uint32_t stage_used;   // staged entries of the chunk
+  uint32_t staged_rows;  // leading rows of the chunk whose runs are staged
+  uint32_t stage_open;   // 0 once a row did not fit
+  uint32_t sub_fit;      // rows of the current sub-tile that were staged
 };
 
 // ---- small helpers -----------------------------------------------------------
@@ -160,7 +164,7 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// ---- tiled path: one C row by a group of g lanes over the tile window ------
+// ---- tiled path ----------------------------------------------------------------
 
 struct TileGeom {
   uint64_t a_base, b_base;
@@ -168,11 +172,10 @@ struct TileGeom {
   uint32_t span;  // staged B rows
   uint64_t base;  // first column of the window (32-aligned)
   uint32_t nwt;   // window words (the last one is always zero)
-  uint32_t sb;    // union block rows (power of two)
-  uint32_t sb_shift;
+  uint32_t sb_shift;  // union block rows = 1 << sb_shift
 };
 
-// OR of the union bitmaps covering A row r on window word w.
+// OR of the union bitmaps covering A row r (sub-tile local) on window word w.
 __device__ __forceinline__ uint32_t tiled_acc(const Smem& S, const TileGeom& T, uint32_t r, uint32_t w) {
   const uint32_t* PRE = S.bits;
   const uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
@@ -223,8 +226,8 @@ __device__ __forceinline__ uint32_t gather_chunk(uint32_t x, bool valid, uint64_
   return total;
 }
 
-// Processes C row r of a tiled tile.  count_only: returns the entry count and
-// adds the row's nnz into nnz_acc (per lane).  Otherwise emits through `emit`.
+// C row r of a tiled sub-tile, window chunk by window chunk.  Returns the
+// entry count; adds the row's nnz into *nnz_acc (per lane) when given.
 template <class Emit>
 __device__ uint32_t tiled_row(const Smem& S, const TileGeom& T, uint32_t r, int g, int lg, unsigned gm,
                               unsigned long long* nnz_acc, Emit&& emit) {
@@ -341,49 +344,92 @@ __device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row
   return count;
 }
 
-// ---- decoupled look-back over the tile ticket order -------------------------
-
-__device__ void lookback(const FusedArgs& p, uint32_t t, unsigned long long cnt, unsigned long long nnz,
-                         unsigned long long& prefix, unsigned long long& prefix_nnz) {
-  TileDesc* d = p.desc;
-  if (t == 0) {
-    prefix = 0;
-    prefix_nnz = 0;
-    d[0].incl_nnz = nnz;
-    st_release(&d[0].incl, kFlag | cnt);
-    return;
-  }
-  d[t].agg_nnz = nnz;
-  st_release(&d[t].agg, kFlag | cnt);
+// ---- warp-parallel decoupled look-back over the chunk order -----------------
+// Called by one full warp; every lane returns the chunk's exclusive prefix.
+__device__ void lookback_warp(const FusedArgs& p, uint32_t t, unsigned long long cnt, unsigned long long nnz,
+                              unsigned long long& prefix, unsigned long long& prefix_nnz) {
+  const int lane = lane_id();
+  ChunkDesc* d = p.desc;
   unsigned long long pre = 0, pre_nnz = 0;
-  int64_t j = int64_t(t) - 1;
-  uint32_t spins = 0;
-  bool timed_out = false;
-  while (j >= 0) {
-    unsigned long long v = ld_acquire(&d[j].incl);
-    if (v & kFlag) {
-      pre += v & ~kFlag;
-      pre_nnz += *reinterpret_cast<volatile unsigned long long*>(&d[j].incl_nnz);
-      break;
+  if (t != 0) {
+    if (lane == 0) {
+      d[t].agg_nnz = nnz;
+      st_release(&d[t].agg, kFlag | cnt);
     }
-    v = ld_acquire(&d[j].agg);
-    if (v & kFlag) {
-      pre += v & ~kFlag;
-      pre_nnz += *reinterpret_cast<volatile unsigned long long*>(&d[j].agg_nnz);
-      --j;
-      continue;
+    int64_t j = int64_t(t) - 1;
+    uint32_t spins = 0;
+    while (true) {
+      const int64_t idx = j - lane;
+      int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: not yet
+      unsigned long long v = 0, vn = 0;
+      if (idx >= 0) {
+        unsigned long long vi = ld_acquire(&d[idx].incl);
+        if (vi & kFlag) {
+          v = vi & ~kFlag;
+          vn = *reinterpret_cast<volatile unsigned long long*>(&d[idx].incl_nnz);
+        } else {
+          unsigned long long va = ld_acquire(&d[idx].agg);
+          if (va & kFlag) {
+            st = 1;
+            v = va & ~kFlag;
+            vn = *reinterpret_cast<volatile unsigned long long*>(&d[idx].agg_nnz);
+          } else {
+            st = 0;
+          }
+        }
+      }
+      const unsigned incl_mask = __ballot_sync(kFullMask, st == 2);
+      const unsigned wait_mask = __ballot_sync(kFullMask, st == 0);
+      const int first = incl_mask ? __ffs(incl_mask) - 1 : 32;
+      const unsigned before = first == 32 ? kFullMask : ((1u << first) - 1u);
+      if (wait_mask & before) {
+        if (++spins > kSpinLimit) {
+          if (lane == 0) atomicOr(&p.ctl->timeout, 1ull);
+          break;
+        }
+        __nanosleep(32);
+        continue;
+      }
+      unsigned long long sv = lane <= first ? v : 0ull, sn = lane <= first ? vn : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sv += __shfl_xor_sync(kFullMask, sv, o);
+        sn += __shfl_xor_sync(kFullMask, sn, o);
+      }
+      pre += sv;
+      pre_nnz += sn;
+      if (first < 32) break;
+      j -= 32;
     }
-    if (++spins > kSpinLimit) {
-      timed_out = true;
-      break;
-    }
-    __nanosleep(64);
   }
-  if (timed_out) atomicOr(&p.ctl->timeout, 1ull);
+  if (lane == 0) {
+    d[t].incl_nnz = pre_nnz + nnz;
+    st_release(&d[t].incl, kFlag | (pre + cnt));
+  }
   prefix = pre;
   prefix_nnz = pre_nnz;
-  d[t].incl_nnz = pre_nnz + nnz;
-  st_release(&d[t].incl, kFlag | (pre + cnt));
+}
+
+// Warp 0: stage offsets for the sub-tile's rows [r0, r0 + rows) whose counts
+// are in S.incl; rows that fit are a prefix of the sub-tile.
+__device__ void stage_rows(Smem& S, uint32_t r0, uint32_t rows) {
+  const int lane = lane_id();
+  const uint32_t v = lane < int(rows) ? S.incl[r0 + lane] : 0u;
+  uint32_t incl = group_incl_sum<32>(kFullMask, v, lane);
+  const uint32_t used = S.stage_used;
+  const bool open = S.stage_open != 0;
+  const bool fits = open && lane < int(rows) && uint64_t(used) + incl <= uint64_t(kStageMax);
+  const unsigned fit_mask = __ballot_sync(kFullMask, fits);
+  const uint32_t nfit = __popc(fit_mask);  // a prefix: incl grows with the lane
+  if (lane < int(rows)) S.sub_off[lane] = used + incl - v;
+  const uint32_t fit_total = nfit ? __shfl_sync(kFullMask, incl, int(nfit) - 1) : 0u;
+  __syncwarp();
+  if (lane == 0) {
+    S.sub_fit = nfit;
+    S.stage_used = used + fit_total;
+    if (nfit < rows) S.stage_open = 0;
+    S.staged_rows += nfit;
+  }
 }
 
 template <bool A_ID>
@@ -393,254 +439,287 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
   while (true) {
-    if (tid == 0) S.tile = atomicAdd(p.ticket, 1u);
+    if (tid == 0) {
+      S.chunk = atomicAdd(p.ticket, 1u);
+      S.stage_used = 0;
+      S.staged_rows = 0;
+      S.stage_open = 1;
+    }
     __syncthreads();
-    const uint32_t t = S.tile;
-    if (t >= p.ntiles) break;
-    const uint32_t i0 = t * kTileRows;
-    const uint32_t rows = min(uint32_t(kTileRows), p.nrows - i0);
-    int mode = kTiled;
-    TileGeom T{};
+    const uint32_t t = S.chunk;
+    if (t >= p.nchunks) break;
+    const uint32_t c0row = t * p.chunk_rows;
+    const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
     unsigned long long nnz_acc = 0;
+    bool any_direct = false;
 
-    // 1. A tile
-    uint64_t a_cnt;
-    if (A_ID) {
-      if (tid <= int(rows)) S.arow[tid] = 2ull * tid;
-      if (tid < int(rows)) S.a[tid] = make_uint2(i0 + tid, i0 + tid);
-      T.a_base = 0;
-      a_cnt = rows;
-    } else {
-      if (tid <= int(rows)) S.arow[tid] = p.a_rowmap[i0 + tid];
-      __syncthreads();
-      T.a_base = S.arow[0];
-      a_cnt = (S.arow[rows] - T.a_base) >> 1;
-      if (a_cnt > kAMax) {
-        mode = kDirect;
+    for (uint32_t r0 = 0; r0 < crows; r0 += kSubRows) {
+      const uint32_t i0 = c0row + r0;
+      const uint32_t rows = min(uint32_t(kSubRows), crows - r0);
+      int mode = kTiled;
+      TileGeom T{};
+
+      // 1. A sub-tile
+      uint64_t a_cnt;
+      if (A_ID) {
+        if (tid <= int(rows)) S.arow[tid] = 2ull * tid;
+        if (tid < int(rows)) S.a[tid] = make_uint2(i0 + tid, i0 + tid);
+        T.a_base = 0;
+        a_cnt = rows;
+        __syncthreads();
       } else {
-        for (uint32_t k = tid; k < a_cnt; k += kThreads) S.a[k] = load_range(p.a_entries, (T.a_base >> 1) + k);
-      }
-    }
-    if (tid == 0) S.stage_used = 0;
-    __syncthreads();
-
-    // 2. B rows named by the tile
-    if (mode == kTiled) {
-      uint32_t mn = 0xffffffffu, mx = 0;
-      for (uint32_t k = tid; k < a_cnt; k += kThreads) {
-        uint2 r = S.a[k];
-        if (r.y >= r.x) {
-          mn = min(mn, r.x);
-          mx = max(mx, r.y);
+        if (tid <= int(rows)) S.arow[tid] = p.a_rowmap[i0 + tid];
+        __syncthreads();
+        T.a_base = S.arow[0];
+        a_cnt = (S.arow[rows] - T.a_base) >> 1;
+        if (a_cnt > kAMax) {
+          mode = kDirect;
+        } else {
+          for (uint32_t k = tid; k < a_cnt; k += kThreads) S.a[k] = load_range(p.a_entries, (T.a_base >> 1) + k);
         }
+        __syncthreads();
       }
-      block_minmax(S, mn, mx);
-      if (mn > mx) {
-        mode = kEmpty;
-      } else {
-        T.bs = mn;
-        T.span = mx - mn + 1;
-        if (T.span > kSpanMax) mode = kDirect;
-      }
-    }
-    if (mode == kTiled) {
-      for (uint32_t k = tid; k <= T.span; k += kThreads) S.brow[k] = p.b_rowmap[uint64_t(T.bs) + k];
-      __syncthreads();
-      T.b_base = S.brow[0];
-      const uint64_t b_cnt = (S.brow[T.span] - T.b_base) >> 1;
-      if (b_cnt > kBMax) {
-        mode = kDirect;
-      } else {
-        for (uint32_t k = tid; k < b_cnt; k += kThreads) S.b[k] = load_range(p.b_entries, (T.b_base >> 1) + k);
-      }
-      __syncthreads();
+
+      // 2. B rows named by the sub-tile, and its column window
       if (mode == kTiled) {
         uint32_t mn = 0xffffffffu, mx = 0;
-        for (uint32_t k = tid; k < b_cnt; k += kThreads) {
-          uint2 r = S.b[k];
+        for (uint32_t k = tid; k < a_cnt; k += kThreads) {
+          uint2 r = S.a[k];
           if (r.y >= r.x) {
             mn = min(mn, r.x);
             mx = max(mx, r.y);
           }
         }
-        uint32_t wmax = 0;  // widest A range (rows)
-        for (uint32_t k = tid; k < a_cnt; k += kThreads) {
-          uint2 r = S.a[k];
-          if (r.y >= r.x) wmax = max(wmax, r.y - r.x + 1);
-        }
         block_minmax(S, mn, mx);
-        uint32_t zero = 0;
-        block_minmax(S, zero, wmax);
         if (mn > mx) {
           mode = kEmpty;
         } else {
-          T.base = mn & ~31u;
-          T.nwt = uint32_t(((uint64_t(mx) - T.base) >> 5) + 2);
-          // union block: about half the widest A range, 2..64 rows
-          uint32_t sb = 2;
-          while (sb < 64 && sb * 4 <= wmax) sb <<= 1;
-          T.sb = sb;
-          T.sb_shift = __ffs(sb) - 1;
-          const uint64_t nblk = (T.span + sb - 1) >> T.sb_shift;
-          const uint64_t need = (2ull * T.span + nblk) * T.nwt;
-          if (need > kBitWords) mode = kDirect;
+          T.bs = mn;
+          T.span = mx - mn + 1;
+          if (T.span > kSpanMax) mode = kDirect;
         }
       }
-    }
-
-    // 3. union bitmaps: R_j into PRE, then SUF (from R) and PRE (in place)
-    if (mode == kTiled) {
-      uint32_t* PRE = S.bits;
-      uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
-      uint32_t* BU = SUF + size_t(T.span) * T.nwt;
-      const uint32_t items = T.span * T.nwt;
-      for (uint32_t it = tid; it < items; it += kThreads) {
-        const uint32_t j = it / T.nwt, w = it - j * T.nwt;
-        PRE[it] = row_mask(S, T.b_base, j, T.base + 32ull * w);
-      }
-      __syncthreads();
-      const uint32_t nblk = (T.span + T.sb - 1) >> T.sb_shift;
-      for (uint32_t it = tid; it < nblk * T.nwt; it += kThreads) {
-        const uint32_t bb = it / T.nwt, w = it - bb * T.nwt;
-        const uint32_t j0 = bb << T.sb_shift, j1 = min(T.span, j0 + T.sb);
-        uint32_t acc = 0;
-        for (uint32_t j = j1; j-- > j0;) {
-          acc |= PRE[size_t(j) * T.nwt + w];
-          SUF[size_t(j) * T.nwt + w] = acc;
-        }
-        acc = 0;
-        for (uint32_t j = j0; j < j1; ++j) {
-          acc |= PRE[size_t(j) * T.nwt + w];
-          PRE[size_t(j) * T.nwt + w] = acc;
-        }
-        BU[size_t(bb) * T.nwt + w] = acc;
-      }
-      __syncthreads();
-
-      // 4. rows: groups of g lanes, each lane one window word per chunk
-      const int g = T.nwt <= 4 ? 4 : T.nwt <= 8 ? 8 : T.nwt <= 16 ? 16 : 32;
-      const int lg = tid & (g - 1);
-      const unsigned gm = runtime_group_mask(g);
-      for (uint32_t r = tid / g; r < rows; r += kThreads / g) {
-        uint32_t slot = 0;
-        uint32_t cnt = 0;
-        if (T.nwt <= uint32_t(g)) {
-          // one chunk: the row stays in registers between count and write
-          const bool valid = uint32_t(lg) < T.nwt;
-          const uint32_t x = valid ? tiled_acc(S, T, r, lg) : 0u;
-          nnz_acc += __popc(x);
-          uint32_t carry = 0;
-          // count first (emit nothing), then write with the slot known
-          uint32_t c2 = carry;
-          cnt = gather_chunk(x, valid, 0, g, lg, gm, c2, 0, T.nwt - 1, [](uint64_t, uint32_t) {});
-          if (lg == 0) slot = atomicAdd(&S.stage_used, cnt);
-          slot = __shfl_sync(gm, slot, 0, g);
-          const bool fits = slot + cnt <= uint32_t(kStageMax);
-          if (fits) {
-            uint32_t* st = S.stage + slot;
-            c2 = 0;
-            gather_chunk(x, valid, T.base + 32ull * lg, g, lg, gm, c2, 0, T.nwt - 1,
-                         [&](uint64_t k, uint32_t v) { st[k] = v; });
-          }
-          if (lg == 0) {
-            S.rcnt[r] = cnt;
-            S.roff[r] = fits ? slot : kNoStage;
-          }
+      if (mode == kTiled) {
+        for (uint32_t k = tid; k <= T.span; k += kThreads) S.brow[k] = p.b_rowmap[uint64_t(T.bs) + k];
+        __syncthreads();
+        T.b_base = S.brow[0];
+        const uint64_t b_cnt = (S.brow[T.span] - T.b_base) >> 1;
+        if (b_cnt > kBMax) {
+          mode = kDirect;
         } else {
-          cnt = tiled_row(S, T, r, g, lg, gm, &nnz_acc, [](uint64_t, uint32_t) {});
-          if (lg == 0) slot = atomicAdd(&S.stage_used, cnt);
-          slot = __shfl_sync(gm, slot, 0, g);
-          const bool fits = slot + cnt <= uint32_t(kStageMax);
-          if (fits) {
-            uint32_t* st = S.stage + slot;
-            tiled_row(S, T, r, g, lg, gm, nullptr, [&](uint64_t k, uint32_t v) { st[k] = v; });
+          for (uint32_t k = tid; k < b_cnt; k += kThreads) S.b[k] = load_range(p.b_entries, (T.b_base >> 1) + k);
+        }
+        __syncthreads();
+        if (mode == kTiled) {
+          uint32_t mn = 0xffffffffu, mx = 0;
+          for (uint32_t k = tid; k < b_cnt; k += kThreads) {
+            uint2 r = S.b[k];
+            if (r.y >= r.x) {
+              mn = min(mn, r.x);
+              mx = max(mx, r.y);
+            }
           }
-          if (lg == 0) {
-            S.rcnt[r] = cnt;
-            S.roff[r] = fits ? slot : kNoStage;
+          uint32_t wmax = 0;  // widest A range (rows)
+          for (uint32_t k = tid; k < a_cnt; k += kThreads) {
+            uint2 r = S.a[k];
+            if (r.y >= r.x) wmax = max(wmax, r.y - r.x + 1);
+          }
+          block_minmax(S, mn, mx);
+          uint32_t zero = 0;
+          block_minmax(S, zero, wmax);
+          if (mn > mx) {
+            mode = kEmpty;
+          } else {
+            T.base = mn & ~31u;
+            T.nwt = uint32_t(((uint64_t(mx) - T.base) >> 5) + 2);
+            // union block: about a quarter of the widest A range, 2..64 rows
+            uint32_t sb = 2;
+            while (sb < 64 && sb * 4 <= wmax) sb <<= 1;
+            T.sb_shift = __ffs(sb) - 1;
+            const uint64_t nblk = (T.span + sb - 1) >> T.sb_shift;
+            if ((2ull * T.span + nblk) * T.nwt > kBitWords) mode = kDirect;
           }
         }
       }
-    } else if (mode == kDirect) {
-      uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
-      uint32_t* reach = bits + kDirectWW;
-      for (uint32_t r = warp; r < rows; r += kWarps) {
-        uint64_t c = direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, &nnz_acc, [](uint64_t, uint32_t) {});
-        if (lane == 0) {
-          S.rcnt[r] = uint32_t(c);
-          S.roff[r] = kNoStage;
-        }
-      }
-    } else {
-      if (tid < int(rows)) {
-        S.rcnt[tid] = 0;
-        S.roff[tid] = 0;
-      }
-    }
-    __syncthreads();
 
-    // 5. tile totals and the look-back
-    const unsigned long long tile_nnz = block_sum(S, nnz_acc);
-    if (warp == 0) {
-      uint32_t v = lane < int(rows) ? S.rcnt[lane] : 0u;
-      uint32_t incl = group_incl_sum<32>(kFullMask, v, lane);
-      if (lane < int(rows)) S.rpre[lane] = incl - v;
-      const unsigned long long tile_cnt = __shfl_sync(kFullMask, incl, 31);
-      if (lane == 0) {
-        unsigned long long pre, pre_nnz;
-        lookback(p, t, tile_cnt, tile_nnz, pre, pre_nnz);
-        S.prefix = pre;
-        if (t == p.ntiles - 1) {
-          p.ctl->total = pre + tile_cnt;
-          p.ctl->nnz = pre_nnz + tile_nnz;
-          if (pre + tile_cnt > p.cap) p.ctl->overflow = pre + tile_cnt;
+      if (mode == kTiled) {
+        // 3. union bitmaps: R_j into PRE, then SUF (from R) and PRE (in place)
+        uint32_t* PRE = S.bits;
+        uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
+        uint32_t* BU = SUF + size_t(T.span) * T.nwt;
+        const uint32_t items = T.span * T.nwt;
+        for (uint32_t it = tid; it < items; it += kThreads) {
+          const uint32_t j = it / T.nwt, w = it - j * T.nwt;
+          PRE[it] = row_mask(S, T.b_base, j, T.base + 32ull * w);
         }
-        if (mode == kDirect) atomicAdd(&p.ctl->tiles_direct, 1ull);
+        __syncthreads();
+        const uint32_t sb = 1u << T.sb_shift;
+        const uint32_t nblk = (T.span + sb - 1) >> T.sb_shift;
+        for (uint32_t it = tid; it < nblk * T.nwt; it += kThreads) {
+          const uint32_t bb = it / T.nwt, w = it - bb * T.nwt;
+          const uint32_t j0 = bb << T.sb_shift, j1 = min(T.span, j0 + sb);
+          uint32_t acc = 0;
+          for (uint32_t j = j1; j-- > j0;) {
+            acc |= PRE[size_t(j) * T.nwt + w];
+            SUF[size_t(j) * T.nwt + w] = acc;
+          }
+          acc = 0;
+          for (uint32_t j = j0; j < j1; ++j) {
+            acc |= PRE[size_t(j) * T.nwt + w];
+            PRE[size_t(j) * T.nwt + w] = acc;
+          }
+          BU[size_t(bb) * T.nwt + w] = acc;
+        }
+        __syncthreads();
+
+        // 4. rows: groups of g lanes, one window word per lane and chunk.
+        // A group holds at most 4 rows (g >= 4 lanes -> >= 8 groups).
+        const int g = T.nwt <= 4 ? 4 : T.nwt <= 8 ? 8 : T.nwt <= 16 ? 16 : 32;
+        const int lg = tid & (g - 1);
+        const unsigned gm = runtime_group_mask(g);
+        const uint32_t gid = tid / g, ngroups = kThreads / g;
+        const bool one_chunk = T.nwt <= uint32_t(g);
+        uint32_t xs[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t r = gid + q * ngroups;
+          xs[q] = 0;
+          if (r < rows) {
+            uint32_t cnt;
+            if (one_chunk) {
+              const bool valid = uint32_t(lg) < T.nwt;
+              const uint32_t x = valid ? tiled_acc(S, T, r, lg) : 0u;
+              xs[q] = x;
+              nnz_acc += __popc(x);
+              uint32_t carry = 0;
+              cnt = gather_chunk(x, valid, 0, g, lg, gm, carry, 0, T.nwt - 1, [](uint64_t, uint32_t) {});
+            } else {
+              cnt = tiled_row(S, T, r, g, lg, gm, &nnz_acc, [](uint64_t, uint32_t) {});
+            }
+            if (lg == 0) S.incl[r0 + r] = cnt;
+          }
+        }
+        __syncthreads();
+        if (warp == 0) stage_rows(S, r0, rows);
+        __syncthreads();
+        const uint32_t fit = S.sub_fit;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t r = gid + q * ngroups;
+          if (r < fit) {
+            uint32_t* st = S.stage + S.sub_off[r];
+            if (one_chunk) {
+              const bool valid = uint32_t(lg) < T.nwt;
+              uint32_t carry = 0;
+              gather_chunk(xs[q], valid, T.base + 32ull * lg, g, lg, gm, carry, 0, T.nwt - 1,
+                           [&](uint64_t k, uint32_t v) { st[k] = v; });
+            } else {
+              tiled_row(S, T, r, g, lg, gm, nullptr, [&](uint64_t k, uint32_t v) { st[k] = v; });
+            }
+          }
+        }
+        __syncthreads();
+      } else if (mode == kDirect) {
+        any_direct = true;
+        uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
+        uint32_t* reach = bits + kDirectWW;
+        for (uint32_t r = warp; r < rows; r += kWarps) {
+          uint64_t c = direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, &nnz_acc, [](uint64_t, uint32_t) {});
+          if (lane == 0) S.incl[r0 + r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+        }
+        __syncthreads();
+        if (warp == 0) stage_rows(S, r0, rows);
+        __syncthreads();
+        const uint32_t fit = S.sub_fit;
+        for (uint32_t r = warp; r < fit; r += kWarps) {
+          uint32_t* st = S.stage + S.sub_off[r];
+          direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) { st[k] = v; });
+        }
+        __syncthreads();
+      } else {
+        if (tid < int(rows)) S.incl[r0 + tid] = 0;
+        __syncthreads();
+        if (warp == 0) stage_rows(S, r0, rows);
+        __syncthreads();
       }
     }
+
+    // 5. chunk prefix over the row counts (8 consecutive rows per thread)
+    {
+      uint32_t loc[8];
+      uint64_t s = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t r = tid * 8 + k;
+        s += r < crows ? S.incl[r] : 0u;
+        loc[k] = uint32_t(s);
+      }
+      // block exclusive scan of the per-thread sums
+      uint64_t inc = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint64_t u = __shfl_up_sync(kFullMask, inc, o);
+        if (lane >= o) inc += u;
+      }
+      if (lane == 31) S.red[warp] = inc;
+      __syncthreads();
+      uint64_t wpre = 0;
+      for (int i = 0; i < warp; ++i) wpre += S.red[i];
+      const uint64_t excl = wpre + inc - s;
+      if (excl + s > 0xffffffffull) atomicOr(&p.ctl->status, 16ull);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t r = tid * 8 + k;
+        if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
+      }
+      __syncthreads();
+    }
+    const unsigned long long chunk_nnz = block_sum(S, nnz_acc);
+    if (warp == 0) {
+      const unsigned long long chunk_cnt = S.incl[crows - 1];
+      unsigned long long pre, pre_nnz;
+      lookback_warp(p, t, chunk_cnt, chunk_nnz, pre, pre_nnz);
+      if (lane == 0) {
+        S.prefix = pre;
+        if (t == p.nchunks - 1) {
+          p.ctl->total = pre + chunk_cnt;
+          p.ctl->nnz = pre_nnz + chunk_nnz;
+          if (pre + chunk_cnt > p.cap) p.ctl->overflow = pre + chunk_cnt;
+        }
+      }
+    }
+    if (tid == 0 && any_direct) atomicAdd(&p.ctl->tiles_direct, 1ull);
     __syncthreads();
     const unsigned long long prefix = S.prefix;
 
-    // 6. rowmap and entries
-    if (tid < int(rows)) p.c_rowmap[uint64_t(i0) + tid + 1] = prefix + S.rpre[tid] + S.rcnt[tid];
+    // 6. rowmap, staged entries, and the rows that did not fit the stage
+    for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
     if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
-    for (uint32_t r = warp; r < rows; r += kWarps) {
-      const uint32_t n = S.rcnt[r];
-      const unsigned long long dst = prefix + S.rpre[r];
-      if (n == 0) continue;
-      if (dst + n > p.cap) {
-        if (lane == 0) atomicOr(&p.ctl->overflow, 1ull);
-        continue;
-      }
-      if (S.roff[r] != kNoStage) {
-        const uint32_t* src = S.stage + S.roff[r];
-        for (uint32_t k = lane; k < n; k += 32) p.c_entries[dst + k] = src[k];
-      } else if (mode == kDirect) {
-        uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
-        uint32_t* reach = bits + kDirectWW;
+    const uint32_t staged = S.stage_used;
+    if (prefix + staged <= p.cap) {
+      for (uint32_t k = tid; k < staged; k += kThreads) p.c_entries[prefix + k] = S.stage[k];
+    } else if (tid == 0) {
+      atomicOr(&p.ctl->overflow, 1ull);
+    }
+    const uint32_t srows = S.staged_rows;
+    if (srows < crows) {
+      uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
+      uint32_t* reach = bits + kDirectWW;
+      for (uint32_t r = srows + warp; r < crows; r += kWarps) {
+        const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+        const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+        if (n == 0) continue;
+        if (dst + n > p.cap) {
+          if (lane == 0) atomicOr(&p.ctl->overflow, 1ull);
+          continue;
+        }
         uint32_t* out = p.c_entries + dst;
         bool bad = false;
-        uint64_t c = direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
+        uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
           if (k < n) out[k] = v;
           else bad = true;
         });
         if (bad || c != n) atomicOr(&p.ctl->status, 8ull);
-      }
-    }
-    if (mode == kTiled) {
-      // rows that did not fit the staging buffer: recompute into global memory
-      const int g = T.nwt <= 4 ? 4 : T.nwt <= 8 ? 8 : T.nwt <= 16 ? 16 : 32;
-      const int lg = tid & (g - 1);
-      const unsigned gm = runtime_group_mask(g);
-      for (uint32_t r = tid / g; r < rows; r += kThreads / g) {
-        if (S.roff[r] != kNoStage || S.rcnt[r] == 0) continue;
-        const uint32_t n = S.rcnt[r];
-        const unsigned long long dst = prefix + S.rpre[r];
-        if (dst + n > p.cap) continue;
-        uint32_t* out = p.c_entries + dst;
-        tiled_row(S, T, r, g, lg, gm, nullptr, [&](uint64_t k, uint32_t v) {
-          if (k < n) out[k] = v;
-        });
       }
     }
     __syncthreads();
@@ -653,8 +732,20 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
                          uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   if (n == 0) return;
-  const uint32_t ntiles = (n + kTileRows - 1) / kTileRows;
-  const size_t desc_bytes = size_t(ntiles) * sizeof(TileDesc);
+  auto kern = a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>;
+  const int smem = int(sizeof(Smem));
+  DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+  if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "fused spgemm: shared memory layout does not fit");
+  const uint64_t resident = uint64_t(per_sm) * ctx->num_sms;
+  // chunk rows: as large as possible (fewer look-back steps) while keeping
+  // about four chunks per resident CTA
+  uint32_t chunk_rows = kChunkMax;
+  while (chunk_rows > kSubRows && (uint64_t(n) + chunk_rows - 1) / chunk_rows < 4 * resident) chunk_rows >>= 1;
+  if (ctx->opt_chunk_rows > 0) chunk_rows = uint32_t(ctx->opt_chunk_rows);
+  const uint32_t nchunks = uint32_t((uint64_t(n) + chunk_rows - 1) / chunk_rows);
+  const size_t desc_bytes = size_t(nchunks) * sizeof(ChunkDesc);
   if (desc_bytes > ctx->tile_desc_cap) {
     if (ctx->d_tile_desc) dfree(ctx, ctx->d_tile_desc);
     ctx->d_tile_desc = nullptr;
@@ -674,18 +765,13 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
   p.c_rowmap = c_rowmap;
   p.c_entries = c_entries;
   p.cap = cap;
-  p.desc = static_cast<TileDesc*>(ctx->d_tile_desc);
+  p.desc = static_cast<ChunkDesc*>(ctx->d_tile_desc);
   p.ticket = ctx->d_ticket;
   p.ctl = ctx->d_ctl;
   p.nrows = n;
-  p.ntiles = ntiles;
-  auto kern = a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>;
-  const int smem = int(sizeof(Smem));
-  DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  int per_sm = 0;
-  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
-  if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "fused spgemm: shared memory layout does not fit");
-  const unsigned grid = unsigned(std::min<uint64_t>(ntiles, uint64_t(per_sm) * ctx->num_sms));
+  p.chunk_rows = chunk_rows;
+  p.nchunks = nchunks;
+  const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
   kern<<<grid, kThreads, smem, ctx->stream>>>(p);
   DVG_CUDA(cudaGetLastError());
   ctx->stats.kernel_launches++;

@@ -81,8 +81,9 @@ dvg_status dvg_synchronize(dvg_context* ctx);
 /* Tuning knobs: "algo" (0 = fused single-pass tile-staged SpGEMM, the
  * default; 1 = two-pass row-direct SpGEMM), "group_lanes" (two-pass path: 0 =
  * autotune, or 4/8/16/32 lanes per output row), "window_words" (two-pass path:
- * 0 = default, else 32-bit accumulator words per row group), "timing" (1 =
- * time kernels with CUDA events into dvg_stats). */
+ * 0 = default, else 32-bit accumulator words per row group), "chunk_rows"
+ * (fused path: 0 = automatic, else rows per output chunk, a multiple of 32 up
+ * to 2048), "timing" (1 = time kernels with CUDA events into dvg_stats). */
 dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value);
 dvg_status dvg_get_stats(const dvg_context* ctx, dvg_stats* out);
 dvg_status dvg_stats_reset(dvg_context* ctx);

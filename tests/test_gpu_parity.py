@@ -24,10 +24,11 @@ def ctx():
     c.close()
 
 
-def set_plan(ctx, plan):
+def set_plan(ctx, plan, chunk_rows=0):
     ctx.set_option("algo", plan[0])
     ctx.set_option("group_lanes", plan[1])
     ctx.set_option("window_words", plan[2])
+    ctx.set_option("chunk_rows", chunk_rows)
 
 
 def as_crs(o):
@@ -127,10 +128,10 @@ def test_banded_spgemm(ctx, plan):
     assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("algo", [0, 1])
+@pytest.mark.parametrize("algo,chunk_rows", [(0, 0), (0, 2048), (1, 0)])
 @pytest.mark.parametrize("window", [(100, 300), (0, 250), (150, 450), (1, 1), (7, 7), (0, 1)])
-def test_small_graph_index(ctx, window, algo):
-    set_plan(ctx, (algo, 0, 0))
+def test_small_graph_index(ctx, window, algo, chunk_rows):
+    set_plan(ctx, (algo, 0, 0), chunk_rows)
     a, _ = gen.graph_adjacency(gen.small_graph_spec(100_000, seed=42))
     want = orc.dindex(omat(a), window[0], window[1], algo="hbv")
     got = ctx.distance_index(ctx.upload(a), *window).download()
@@ -156,29 +157,33 @@ def spgemm_case(ctx, a, b, expect_direct=None):
     return ctx.stats()
 
 
-def test_fused_tiled_single_chunk_and_stage_overflow(ctx):
-    # narrow band, many short output runs: staged tiles whose output exceeds
-    # the staging buffer and is recomputed into global memory
-    set_plan(ctx, (0, 0, 0))
+@pytest.mark.parametrize("chunk_rows", [0, 32, 256, 2048])
+def test_fused_tiled_single_chunk_and_stage_overflow(ctx, chunk_rows):
+    # narrow band, many short output runs: staged sub-tiles; with large chunks
+    # the output outgrows the staging area and the remaining rows are
+    # recomputed into global memory
+    set_plan(ctx, (0, 0, 0), chunk_rows)
     a = gen.banded(20_000, 20, 3.0, 1.0, seed=41)
     b = gen.banded(20_000, 300, 10.0, 1.0, seed=42)
     st = spgemm_case(ctx, a, b)
     assert st["spgemm_direct_tiles"] == 0
 
 
-def test_fused_tiled_multi_chunk(ctx):
-    # a tile window wider than 32 words: lane groups loop over window chunks
-    set_plan(ctx, (0, 0, 0))
+@pytest.mark.parametrize("chunk_rows", [0, 2048])
+def test_fused_tiled_multi_chunk(ctx, chunk_rows):
+    # a sub-tile window wider than 32 words: lane groups loop over window chunks
+    set_plan(ctx, (0, 0, 0), chunk_rows)
     a = gen.banded(20_000, 20, 3.0, 1.0, seed=43)
-    b = gen.banded(20_000, 600, 10.0, 1.0, seed=44)
+    b = gen.banded(20_000, 500, 6.0, 1.0, seed=44)
     st = spgemm_case(ctx, a, b)
     assert st["spgemm_direct_tiles"] == 0
 
 
-def test_fused_direct_tiles_and_capacity_rerun(ctx):
-    # random columns: every tile misses the staged path; the output exceeds the
-    # speculative capacity, which is detected and re-run at the exact size
-    set_plan(ctx, (0, 0, 0))
+@pytest.mark.parametrize("chunk_rows", [0, 64, 2048])
+def test_fused_direct_tiles_and_capacity_rerun(ctx, chunk_rows):
+    # random columns: every sub-tile misses the staged path; the output exceeds
+    # the speculative capacity, which is detected and re-run at the exact size
+    set_plan(ctx, (0, 0, 0), chunk_rows)
     a = gen.random_matrix(2000, 8000, seed=45)
     b = gen.random_matrix(2000, 30000, seed=46)
     st = spgemm_case(ctx, a, b)
