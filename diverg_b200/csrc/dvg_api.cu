@@ -47,6 +47,8 @@ struct Lock {
 
 namespace dvg {
 
+void record_error(const std::string& msg) { g_last_error = msg; }
+
 void cuda_check(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return;
   dvg_status s = (e == cudaErrorMemoryAllocation) ? DVG_ERR_OOM : DVG_ERR_DEVICE;

@@ -75,6 +75,8 @@ struct Error : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char* what);
+// Sets the message dvg_last_error() returns on the calling thread.
+void record_error(const std::string& msg);
 #define DVG_CUDA(call) ::dvg::cuda_check((call), #call)
 
 void* dalloc(dvg_context* ctx, size_t bytes);

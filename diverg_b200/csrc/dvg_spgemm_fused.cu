@@ -32,6 +32,7 @@
 // direct path straight into global memory after the look-back.  Look-back
 // waits are bounded: on expiry the kernel records a timeout.
 #include <algorithm>
+#include <mutex>
 
 #include "dvg_device.cuh"
 #include "dvg_internal.h"
@@ -778,3 +779,171 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
 }
 
 }  // namespace dvg
+
+// ---- the no-allocation entry point -------------------------------------------
+//
+// dvg_range_spgemm_noalloc runs the fused kernel above for callers that may
+// not allocate device memory.  Its chunk descriptors, tile ticket and control
+// block live in one file-scope device array, sized for kNoAllocMaxChunks
+// chunks of at most kChunkMax rows, i.e. products with up to
+// kNoAllocMaxChunks * kChunkMax = 67,108,864 output rows.  Every GPU that
+// loads the library holds this array (about 1 MiB) until the process exits.
+// All calls share it and it keeps the last call's contents, so each call
+// clears the part it uses before its kernels run; calls whose work overlaps
+// on the GPU (from several streams or threads) race on it and must be
+// serialised by the caller.
+namespace dvg {
+namespace {
+
+constexpr uint32_t kNoAllocMaxChunks = 32768;
+constexpr size_t kNoAllocDescBytes = size_t(kNoAllocMaxChunks) * sizeof(ChunkDesc);
+constexpr size_t kNoAllocCtlOffset = kNoAllocDescBytes;                 // DeviceControl
+constexpr size_t kNoAllocTicketOffset = kNoAllocCtlOffset + 256;       // tile ticket
+constexpr size_t kNoAllocBytes = kNoAllocTicketOffset + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch per device ordinal.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device (with that device current) and cached here.
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Sets bit 1 of *bad when a range-CRS matrix violates the memory-safety
+// preconditions of the fused kernel (rowmap[0] = 0, non-decreasing, even row
+// lengths, rowmap[n] = nentries, columns < ncols).
+__global__ void k_noalloc_validate(const uint64_t* __restrict__ rowmap, uint32_t nrows,
+                                   const uint32_t* __restrict__ entries, uint64_t nentries, uint32_t ncols,
+                                   unsigned long long* bad) {
+  unsigned long long b = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  for (uint64_t i = tid; i < nrows; i += stride) {
+    const uint64_t lo = rowmap[i], hi = rowmap[i + 1];
+    if (hi < lo || ((hi - lo) & 1)) b = 1;
+  }
+  if (tid == 0 && (rowmap[0] != 0 || rowmap[nrows] != nentries)) b = 1;
+  for (uint64_t i = tid; i < nentries; i += stride)
+    if (entries[i] >= ncols) b = 1;
+  if (b) atomicOr(bad, 1ull);
+}
+
+dvg_status dvg_noalloc_fail(dvg_status s, const std::string& msg) {
+  record_error(msg);
+  return s;
+}
+
+}  // namespace
+}  // namespace dvg
+
+extern "C" dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncols, const uint64_t* d_a_rowmap,
+                                               const uint32_t* d_a_entries, uint64_t a_nentries, uint32_t b_nrows,
+                                               uint32_t b_ncols, const uint64_t* d_b_rowmap,
+                                               const uint32_t* d_b_entries, uint64_t b_nentries,
+                                               uint64_t* d_c_rowmap, uint32_t* d_c_entries, uint64_t c_capacity,
+                                               uint64_t* c_nentries, uint64_t* c_nnz, void* cuda_stream) {
+  using namespace dvg;
+  // Argument checks come first and touch no pointer, so an oversized request
+  // is rejected before any device work.
+  if (!c_nentries || !c_nnz) return dvg_noalloc_fail(DVG_ERR_INVALID_ARG, "null output pointer");
+  *c_nentries = 0;
+  *c_nnz = 0;
+  if (uint64_t(a_nrows) > uint64_t(kNoAllocMaxChunks) * kChunkMax)
+    return dvg_noalloc_fail(DVG_ERR_INVALID_ARG,
+                            "dvg_range_spgemm_noalloc: more than 67108864 output rows (its scratch limit); "
+                            "use dvg_range_spgemm");
+  if (a_ncols != b_nrows) return dvg_noalloc_fail(DVG_ERR_INVALID_ARG, "a.numCols() != b.numRows()");
+  if (a_ncols > 0xFFFFFFFEu || b_ncols > 0xFFFFFFFEu)
+    return dvg_noalloc_fail(DVG_ERR_INVALID_ARG, "ncols must be below 2^32 - 1");
+  if (!d_a_rowmap || !d_b_rowmap || !d_c_rowmap || (a_nentries && !d_a_entries) || (b_nentries && !d_b_entries) ||
+      (c_capacity && !d_c_entries))
+    return dvg_noalloc_fail(DVG_ERR_INVALID_ARG, "null device pointer");
+  if ((reinterpret_cast<uintptr_t>(d_a_entries) | reinterpret_cast<uintptr_t>(d_b_entries)) & 7)
+    return dvg_noalloc_fail(DVG_ERR_INVALID_ARG, "entries must be 8-byte aligned");
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  try {
+    int dev = 0;
+    DVG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error(DVG_ERR_DEVICE, "device ordinal out of range");
+    unsigned char* scratch = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(g_noalloc_mu);
+      if (!g_noalloc_ptr[dev]) {
+        void* ptr = nullptr;
+        DVG_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = ptr;
+      }
+      scratch = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+    }
+    ChunkDesc* desc = reinterpret_cast<ChunkDesc*>(scratch);
+    DeviceControl* ctl = reinterpret_cast<DeviceControl*>(scratch + kNoAllocCtlOffset);
+    unsigned* ticket = reinterpret_cast<unsigned*>(scratch + kNoAllocTicketOffset);
+    DeviceControl h{};
+    if (a_nrows == 0) {
+      DVG_CUDA(cudaMemsetAsync(d_c_rowmap, 0, sizeof(uint64_t), stream));
+      DVG_CUDA(cudaStreamSynchronize(stream));
+      return DVG_OK;
+    }
+    // 1. inputs must be well formed before the product may index through them
+    int nsm = 0;
+    DVG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    DVG_CUDA(cudaMemsetAsync(ctl, 0, sizeof(DeviceControl), stream));
+    const unsigned vgrid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(
+        (std::max<uint64_t>(std::max<uint64_t>(a_nrows, a_nentries), std::max<uint64_t>(b_nrows, b_nentries)) +
+         255) / 256, uint64_t(nsm) * 8)));
+    k_noalloc_validate<<<vgrid, 256, 0, stream>>>(d_a_rowmap, a_nrows, d_a_entries, a_nentries, a_ncols,
+                                                  &ctl->invalid);
+    k_noalloc_validate<<<vgrid, 256, 0, stream>>>(d_b_rowmap, b_nrows, d_b_entries, b_nentries, b_ncols,
+                                                  &ctl->invalid);
+    DVG_CUDA(cudaGetLastError());
+    DVG_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, stream));
+    DVG_CUDA(cudaStreamSynchronize(stream));
+    if (h.invalid) throw Error(DVG_ERR_INVALID_ARG, "malformed range-CRS input matrix");
+    // 2. the fused product with this file's scratch
+    auto kern = k_spgemm_fused<false>;
+    const int smem = int(sizeof(Smem));
+    DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+    if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "fused spgemm: shared memory layout does not fit");
+    const uint64_t resident = uint64_t(per_sm) * nsm;
+    uint32_t chunk_rows = kChunkMax;
+    while (chunk_rows > kSubRows && (uint64_t(a_nrows) + chunk_rows - 1) / chunk_rows < 4 * resident)
+      chunk_rows >>= 1;
+    const uint32_t nchunks = uint32_t((uint64_t(a_nrows) + chunk_rows - 1) / chunk_rows);
+    if (nchunks > kNoAllocMaxChunks) throw Error(DVG_ERR_INVALID_ARG, "too many output chunks for the scratch");
+    DVG_CUDA(cudaMemsetAsync(desc, 0, size_t(nchunks) * sizeof(ChunkDesc), stream));
+    DVG_CUDA(cudaMemsetAsync(ctl, 0, sizeof(DeviceControl), stream));
+    DVG_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), stream));
+    FusedArgs p{};
+    p.a_rowmap = d_a_rowmap;
+    p.a_entries = d_a_entries;
+    p.b_rowmap = d_b_rowmap;
+    p.b_entries = d_b_entries;
+    p.c_rowmap = d_c_rowmap;
+    p.c_entries = d_c_entries;
+    p.cap = c_capacity;
+    p.desc = desc;
+    p.ticket = ticket;
+    p.ctl = ctl;
+    p.nrows = a_nrows;
+    p.chunk_rows = chunk_rows;
+    p.nchunks = nchunks;
+    const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
+    kern<<<grid, kThreads, smem, stream>>>(p);
+    DVG_CUDA(cudaGetLastError());
+    DVG_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, stream));
+    DVG_CUDA(cudaStreamSynchronize(stream));
+    *c_nentries = h.total;
+    *c_nnz = h.nnz;
+    if (h.timeout) throw Error(DVG_ERR_TIMEOUT, "range_spgemm: chunk look-back wait expired");
+    if (h.status) throw Error(DVG_ERR_DEVICE, "internal consistency check failed on the device");
+    if (h.overflow)
+      throw Error(DVG_ERR_OVERFLOW, "c_capacity is smaller than the product's " + std::to_string(h.total) +
+                                        " entries (c_rowmap is complete; call again with a larger buffer)");
+  } catch (const Error& e) {
+    return dvg_noalloc_fail(e.status, e.what());
+  }
+  return DVG_OK;
+}

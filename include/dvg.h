@@ -130,6 +130,35 @@ dvg_status dvg_range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k, dv
 dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, unsigned dmin, unsigned dmax,
                                      dvg_matrix** out);
 
+/* ---- range SpGEMM without device allocation -------------------------------
+ * No counterpart in the reference.  Some callers of this library cannot let it
+ * allocate device memory: a server that reserves the GPU's memory for resident
+ * indices up front and hands out buffers from its own pool, a host runtime
+ * (a JVM, a database engine) that owns every device allocation through its
+ * own allocator, and latency-critical paths where cudaMalloc/cudaFree would
+ * synchronise the device.  This entry point computes C = A * B exactly as
+ * dvg_range_spgemm does, from caller-owned device arrays into caller-owned
+ * device arrays, and allocates nothing: no cudaMalloc, no cudaFree, no
+ * allocating library call.  It needs no dvg_context.
+ *
+ * Its scratch is a fixed array inside the library (about 1 MiB, held on every
+ * GPU that loads the library until the process exits), which limits the
+ * product to a_nrows <= 67,108,864; larger products are rejected with
+ * DVG_ERR_INVALID_ARG.  The first call on a device looks up that array's
+ * device address; make this first call before any stream capture.  All calls
+ * share the array: calls whose work overlaps on the GPU race and must be
+ * serialised by the caller.
+ *
+ * d_c_rowmap holds a_nrows + 1 entries; d_c_entries holds c_capacity entries.
+ * On return *c_nentries and *c_nnz describe C.  If c_capacity is too small
+ * the call returns DVG_ERR_OVERFLOW with c_rowmap complete and *c_nentries
+ * set to the required capacity.  The call synchronises `cuda_stream`. */
+dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncols, const uint64_t* d_a_rowmap,
+                                    const uint32_t* d_a_entries, uint64_t a_nentries, uint32_t b_nrows,
+                                    uint32_t b_ncols, const uint64_t* d_b_rowmap, const uint32_t* d_b_entries,
+                                    uint64_t b_nentries, uint64_t* d_c_rowmap, uint32_t* d_c_entries,
+                                    uint64_t c_capacity, uint64_t* c_nentries, uint64_t* c_nnz, void* cuda_stream);
+
 /* ---- membership query: crs_matrix.hpp:1197-1243 (operator() / at) -------- */
 
 /* out[q] = index(pairs[2q], pairs[2q+1]) as 0/1 for q < npairs; device
