@@ -293,7 +293,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": None,
                 "peak_kind": peak_kind,
-                "kernel": "k_spgemm_rows (symbolic + numeric passes of one range SpGEMM)",
+                "kernel": "k_spgemm_rowmode (single-pass range SpGEMM: counts, chunk look-back, runs)",
                 "alg_bytes_per_product": per_product_bytes, "products_per_build": st["spgemm_calls"] / args.steps}
 
     cpu = None

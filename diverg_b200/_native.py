@@ -28,7 +28,8 @@ class DvgStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "kernel_launches", "spgemm_calls", "spadd_calls", "host_syncs", "alg_bytes",
         "spgemm_alg_bytes", "range_ops", "h2d_bytes", "d2h_bytes", "spgemm_symbolic_ns", "spgemm_numeric_ns",
-        "scan_ns", "spadd_ns", "spgemm_direct_tiles", "spgemm_reruns")]
+        "scan_ns", "spadd_ns", "spgemm_direct_tiles", "spgemm_reruns", "spgemm_light", "spgemm_slow_rows", "host_alloc_ns",
+        "host_sync_ns")]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
@@ -61,6 +62,7 @@ DVG_SIGNATURES = {
     "dvg_set_stream": [_P, _P],
     "dvg_synchronize": [_P],
     "dvg_set_option": [_P, ctypes.c_char_p, _I64],
+    "dvg_trim": [_P],
     "dvg_get_stats": [_P, ctypes.POINTER(DvgStats)],
     "dvg_stats_reset": [_P],
     "dvg_last_error": [],

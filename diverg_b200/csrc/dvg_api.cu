@@ -2,6 +2,7 @@
 // range operations: products, sums, powers and the distance index.  Every
 // entry point converts internal failures into a dvg_status.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -55,20 +56,63 @@ void cuda_check(cudaError_t e, const char* what) {
   throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+static uint64_t now_ns() {
+  return uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(
+                      std::chrono::steady_clock::now().time_since_epoch()).count());
+}
+
+// Returns every cached block to the stream-ordered pool.
+static void release_cached(dvg_context* ctx) {
+  for (auto& kv : ctx->free_blocks) DVG_CUDA(cudaFreeAsync(kv.second, ctx->stream));
+  ctx->free_blocks.clear();
+  ctx->cached_bytes = 0;
+}
+
+// Device allocation for the context's stream.  A freed block whose size is
+// within [bytes, bytes + bytes/4] is reused (best fit); otherwise the request
+// goes to cudaMallocAsync, and when that fails the cache is released and the
+// request retried once.  Re-mapping GB-sized buffers in the pool on every
+// product costs tens to hundreds of milliseconds per index build.
 void* dalloc(dvg_context* ctx, size_t bytes) {
+  const uint64_t t0 = now_ns();
+  bytes = (std::max<size_t>(bytes, 16) + 255) & ~size_t(255);
+  auto it = ctx->free_blocks.lower_bound(bytes);
+  if (it != ctx->free_blocks.end() && it->first <= bytes + bytes / 4) {
+    void* p = it->second;
+    ctx->live_blocks[p] = it->first;
+    ctx->cached_bytes -= it->first;
+    ctx->free_blocks.erase(it);
+    ctx->stats.host_alloc_ns += now_ns() - t0;
+    return p;
+  }
   void* p = nullptr;
-  if (bytes == 0) bytes = 16;
   cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+  if (e == cudaErrorMemoryAllocation && !ctx->free_blocks.empty()) {
+    (void)cudaGetLastError();
+    release_cached(ctx);
+    DVG_CUDA(cudaStreamSynchronize(ctx->stream));
+    e = cudaMallocAsync(&p, bytes, ctx->stream);
+  }
+  ctx->stats.host_alloc_ns += now_ns() - t0;
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     throw Error(e == cudaErrorMemoryAllocation ? DVG_ERR_OOM : DVG_ERR_DEVICE,
                 std::string("device allocation of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
   }
+  ctx->live_blocks[p] = bytes;
   return p;
 }
 
 void dfree(dvg_context* ctx, void* p) {
-  if (p) DVG_CUDA(cudaFreeAsync(p, ctx->stream));
+  if (!p) return;
+  auto it = ctx->live_blocks.find(p);
+  if (it == ctx->live_blocks.end()) {
+    DVG_CUDA(cudaFreeAsync(p, ctx->stream));
+    return;
+  }
+  ctx->free_blocks.emplace(it->second, p);
+  ctx->cached_bytes += it->second;
+  ctx->live_blocks.erase(it);
 }
 
 static size_t entries_alloc_bytes(uint64_t nentries) {
@@ -150,7 +194,9 @@ void reset_control(dvg_context* ctx) {
 
 DeviceControl read_control(dvg_context* ctx) {
   DVG_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, ctx->stream));
+  const uint64_t t0 = now_ns();
   DVG_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->stats.host_sync_ns += now_ns() - t0;
   ctx->stats.host_syncs++;
   resolve_spans(ctx);
   DeviceControl c = *ctx->h_ctl;
@@ -194,8 +240,10 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
     }
     c->nentries = ctl.total;
     c->nnz = ctl.nnz;
+    c->canonical = true;
     ctx->stats.spgemm_calls++;
     ctx->stats.spgemm_direct_tiles += ctl.tiles_direct;
+    ctx->stats.spgemm_slow_rows += ctl.slow_rows;
     uint64_t bytes = (a_identity ? 0 : matrix_bytes(a)) + matrix_bytes(b) + matrix_bytes(c);
     ctx->stats.alg_bytes += bytes;
     ctx->stats.spgemm_alg_bytes += bytes;
@@ -275,6 +323,7 @@ dvg_matrix* range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix*
       span_end(ctx, t0, kSpadd);
     }
     c->nnz = ctl.nnz;
+    c->canonical = a->canonical && (b_identity || b->canonical);
     ctx->stats.spadd_calls++;
     ctx->stats.alg_bytes += matrix_bytes(a) + (b_identity ? 0 : matrix_bytes(b)) + matrix_bytes(c);
   } catch (...) {
@@ -326,10 +375,10 @@ dvg_matrix* range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k) {
   return c;
 }
 
-// util::create_distance_index, dindex.hpp:46-189.
-dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup) {
-  require(dlo <= dup && dup != 0, "create_distance_index: requires dmin <= dmax and dmax != 0");
-  require(a->nrows == a->ncols, "create_distance_index: adjacency matrix is not square");
+// util::create_distance_index, dindex.hpp:46-189, as the reference
+// schedules it: rai = I + A; rad = A^dlo and raid = rai^(dup-dlo) by
+// square-and-multiply; d = rad * raid.
+static dvg_matrix* distance_index_reference(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup) {
   dvg_matrix* rai = range_spadd(ctx, a, nullptr, true);  // I + A (fused identity)
   dvg_matrix* rad = nullptr;
   dvg_matrix* raid = nullptr;
@@ -353,6 +402,127 @@ dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigne
     throw;
   }
   return d;
+}
+
+// The same index, T = A^dlo * (A+I)^K with K = dup - dlo, scheduled so that
+// every product has a power of A -- whose rows hold a few narrow ranges -- as
+// its left operand.  Over the Boolean semiring (A+I)^n = sum_{j<=n} A^j, so
+//   (A+I)^(a+b) = (A+I)^a + A^a (A+I)^b     for every Boolean matrix A.
+// With P_m = A^(2^m) (square A) and Q_m = (A+I)^(2^m):
+//   Q_0 = A + I,  Q_(m+1) = Q_m + P_m Q_m,
+// (A+I)^K is assembled over the set bits of K with the same identity, and
+// A^dlo by square-and-multiply over the P_m.  T is the same canonical matrix
+// as the reference's A^dlo * (A+I)^K (both equal sum_{dlo<=j<=dup} A^j), so
+// the output is identical, while the wide-row squarings of (A+I)^k -- whose
+// rows name ~k B rows each -- are gone.
+static dvg_matrix* distance_index_powersum(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup) {
+  const unsigned K = dup - dlo;
+  std::vector<dvg_matrix*> P;  // P[m] = A^(2^m); P[0] is `a` (not owned)
+  std::vector<dvg_matrix*> owned;
+  auto own = [&](dvg_matrix* m) {
+    owned.push_back(m);
+    return m;
+  };
+  auto release = [&](dvg_matrix* m) {
+    for (auto& o : owned)
+      if (o == m) {
+        free_matrix(ctx, o);
+        o = nullptr;
+      }
+  };
+  int top_k = -1, top_lo = -1;
+  for (int b = 31; b >= 0; --b) {
+    if (top_k < 0 && (K >> b) & 1u) top_k = b;
+    if (top_lo < 0 && (dlo >> b) & 1u) top_lo = b;
+  }
+  const int need_p = std::max(top_k, top_lo);  // highest P_m used
+  try {
+    P.push_back(const_cast<dvg_matrix*>(a));
+    for (int m = 1; m <= need_p; ++m) P.push_back(own(range_spgemm(ctx, P[m - 1], false, P[m - 1])));
+
+    // (A+I)^K
+    dvg_matrix* R = nullptr;   // (A+I)^e, e = sum of the bits of K handled so far
+    dvg_matrix* Ae = nullptr;  // A^e (nullptr: e has one bit, A^e = P[that bit])
+    unsigned e = 0;
+    if (K == 0) {
+      R = own(identity(ctx, a->ncols));
+    } else {
+      dvg_matrix* Q = own(range_spadd(ctx, a, nullptr, true));  // Q_0 = A + I
+      for (int m = 0; m <= top_k; ++m) {
+        if ((K >> m) & 1u) {
+          if (!R) {
+            R = Q;
+            e = 1u << m;
+          } else {
+            // (A+I)^(e + 2^m) = (A+I)^e + A^e Q_m
+            const dvg_matrix* Aexp = Ae ? Ae : P[__builtin_ctz(e)];
+            dvg_matrix* t = own(range_spgemm(ctx, Aexp, false, Q));
+            dvg_matrix* nr = own(range_spadd(ctx, R, t, false));
+            release(t);
+            if (R != Q) release(R);
+            R = nr;
+            // A^(e + 2^m) = A^e P_m, needed only for a later bit
+            if ((K >> (m + 1)) != 0) {
+              dvg_matrix* na = own(range_spgemm(ctx, Aexp, false, P[m]));
+              if (Ae) release(Ae);
+              Ae = na;
+            }
+            e += 1u << m;
+          }
+        }
+        if (m < top_k) {
+          // Q_(m+1) = Q_m + P_m Q_m
+          dvg_matrix* t = own(range_spgemm(ctx, P[m], false, Q));
+          dvg_matrix* nq = own(range_spadd(ctx, Q, t, false));
+          release(t);
+          if (Q != R) release(Q);
+          Q = nq;
+        }
+      }
+      if (Q != R) release(Q);
+      if (Ae) release(Ae);
+    }
+
+    // A^dlo by square-and-multiply over the P_m, then T = A^dlo (A+I)^K
+    dvg_matrix* T = nullptr;
+    if (dlo == 0) {
+      T = R;
+    } else {
+      dvg_matrix* Ad = nullptr;  // nullptr: a single P_m so far
+      int first = -1;
+      for (int m = 0; m <= top_lo; ++m) {
+        if (!((dlo >> m) & 1u)) continue;
+        if (first < 0) {
+          first = m;
+        } else {
+          dvg_matrix* n2 = own(range_spgemm(ctx, Ad ? Ad : P[first], false, P[m]));
+          if (Ad) release(Ad);
+          Ad = n2;
+        }
+      }
+      T = range_spgemm(ctx, Ad ? Ad : P[first], false, R);
+      if (Ad) release(Ad);
+      release(R);
+    }
+    for (auto& o : owned)
+      if (o && o != T) free_matrix(ctx, o);
+    owned.clear();
+    return T;
+  } catch (...) {
+    for (auto& o : owned)
+      if (o) free_matrix(ctx, o);
+    throw;
+  }
+}
+
+dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup) {
+  require(dlo <= dup && dup != 0, "create_distance_index: requires dmin <= dmax and dmax != 0");
+  require(a->nrows == a->ncols, "create_distance_index: adjacency matrix is not square");
+  // the sum-of-powers schedule ends on SpAdds when dlo == 0; those keep rows
+  // canonical only for canonical inputs, while the reference's squarings
+  // canonicalise any input
+  if (ctx->opt_dindex_schedule == 1 || (dlo == 0 && !a->canonical)) return distance_index_reference(ctx, a, dlo, dup);
+  return distance_index_powersum(ctx, a, dlo, dup);
 }
 
 }  // namespace dvg
@@ -422,6 +592,7 @@ dvg_status dvg_shutdown(dvg_context* ctx) {
     if (ctx->d_answers) dfree(ctx, ctx->d_answers);
     if (ctx->d_tile_desc) dfree(ctx, ctx->d_tile_desc);
     if (ctx->d_ticket) dfree(ctx, ctx->d_ticket);
+    release_cached(ctx);
     DVG_CUDA(cudaStreamSynchronize(ctx->stream));
     resolve_spans(ctx);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
@@ -464,6 +635,12 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "algo")) {
       require(value == 0 || value == 1, "algo must be 0 (fused tiled) or 1 (two-pass direct)");
       ctx->opt_algo = value;
+    } else if (!std::strcmp(key, "dindex_schedule")) {
+      require(value == 0 || value == 1, "dindex_schedule must be 0 (sum of powers) or 1 (reference squaring)");
+      ctx->opt_dindex_schedule = value;
+    } else if (!std::strcmp(key, "spgemm_mode")) {
+      require(value >= 0 && value <= 2, "spgemm_mode must be 0 (automatic), 1 (tiled) or 2 (light)");
+      ctx->opt_spgemm_mode = value;
     } else if (!std::strcmp(key, "chunk_rows")) {
       require(value >= 0 && value <= 2048 && value % 32 == 0, "chunk_rows must be 0 or a multiple of 32 up to 2048");
       ctx->opt_chunk_rows = value;
@@ -474,6 +651,14 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else {
       require(false, "unknown option");
     }
+  });
+}
+
+dvg_status dvg_trim(dvg_context* ctx) {
+  return guarded([&] {
+    Lock lk(ctx);
+    release_cached(ctx);
+    DVG_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 
@@ -494,6 +679,8 @@ static void validate_uploaded(dvg_context* ctx, dvg_matrix* m) {
   reset_control(ctx);
   launch_validate(ctx, m->rowmap, m->nrows, m->entries, m->nentries, m->ncols);
   DeviceControl c = read_control(ctx);
+  m->canonical = !(c.invalid & 16);
+  c.invalid &= ~16ull;
   if (c.invalid) {
     std::string why;
     if (c.invalid & 1) why += " rowmap[0] != 0;";

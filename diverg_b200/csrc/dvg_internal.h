@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <unordered_map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -20,6 +22,7 @@ struct dvg_matrix {
   uint64_t* rowmap = nullptr;   // device, nrows + 1
   uint32_t* entries = nullptr;  // device, nentries (allocation padded to 16 B)
   bool owned = true;
+  bool canonical = true;  // rows sorted, disjoint and non-adjacent (as SpGEMM emits them)
   int device = 0;
 };
 
@@ -33,6 +36,7 @@ struct DeviceControl {
   unsigned long long overflow;   // nonzero: the fused product exceeded its capacity
   unsigned long long timeout;    // nonzero: a bounded device wait gave up
   unsigned long long tiles_direct;  // tiles that took the direct (unstaged) path
+  unsigned long long slow_rows;     // row-mode rows that missed the shared window
 };
 
 struct dvg_context {
@@ -56,6 +60,8 @@ struct dvg_context {
   int64_t opt_window_words = 0;
   int64_t opt_algo = 0;               // 0: fused tiled SpGEMM, 1: two-pass direct
   int64_t opt_chunk_rows = 0;         // fused SpGEMM look-back chunk rows (0: automatic)
+  int64_t opt_spgemm_mode = 0;        // fused SpGEMM: 0 automatic, 1 tiled, 2 light
+  int64_t opt_dindex_schedule = 0;    // 0: sum of powers, 1: the reference's squaring
   bool opt_timing = false;
   // event pairs bracketing timed kernels, resolved at the next stream sync
   struct TimedSpan {
@@ -64,6 +70,11 @@ struct dvg_context {
   };
   std::vector<TimedSpan> timed;
   std::vector<cudaEvent_t> event_pool;
+  // caching allocator: blocks freed by the context are kept (stream order
+  // makes their reuse on the context's stream safe) and handed out again
+  std::multimap<size_t, void*> free_blocks;      // bytes -> block
+  std::unordered_map<void*, size_t> live_blocks;  // block -> bytes
+  size_t cached_bytes = 0;
 };
 
 namespace dvg {

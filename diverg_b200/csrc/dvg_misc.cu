@@ -28,7 +28,9 @@ __global__ void k_identity(uint64_t* __restrict__ rowmap, uint32_t* __restrict__
 
 // ---- validation: the memory-safety preconditions of every kernel ----------
 // bit 1: rowmap[0] != 0; bit 2: rowmap decreasing or odd row length;
-// bit 4: rowmap[n] != nentries; bit 8: an entry >= ncols.
+// bit 4: rowmap[n] != nentries; bit 8: an entry >= ncols.  Not an error:
+// bit 16 marks a matrix whose rows are not canonical (a range with end <
+// start, or a range that does not start past the previous range's end + 1).
 __global__ void k_validate(const uint64_t* __restrict__ rowmap, uint32_t nrows, const uint32_t* __restrict__ entries,
                            uint64_t nentries, uint32_t ncols, DeviceControl* ctl) {
   unsigned long long bad = 0;
@@ -36,7 +38,14 @@ __global__ void k_validate(const uint64_t* __restrict__ rowmap, uint32_t nrows, 
   const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
   for (uint64_t i = tid; i < nrows; i += stride) {
     uint64_t a = rowmap[i], b = rowmap[i + 1];
-    if (b < a || ((b - a) & 1)) bad |= 2;
+    if (b < a || ((b - a) & 1)) {
+      bad |= 2;
+    } else if (b <= nentries) {
+      for (uint64_t k = a; k < b; k += 2) {
+        if (entries[k + 1] < entries[k] || (k > a && uint64_t(entries[k]) <= uint64_t(entries[k - 1]) + 1))
+          bad |= 16;
+      }
+    }
   }
   if (tid == 0) {
     if (rowmap[0] != 0) bad |= 1;

@@ -40,20 +40,25 @@
 namespace dvg {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSubRows = 32;      // rows per staged sub-tile
+constexpr int kSubRows = 64;      // rows per staged sub-tile
 constexpr int kChunkMax = 2048;   // rows per look-back chunk (upper bound)
-constexpr int kAMax = 256;        // A ranges staged per sub-tile
-constexpr int kSpanMax = 512;     // B rows staged per sub-tile
-constexpr int kBMax = 1024;       // B ranges staged per sub-tile
-constexpr int kBitWords = 7168;   // union bitmaps (PRE, SUF, BU) or direct windows
+constexpr int kSubMax = kChunkMax / kSubRows;
+constexpr int kAChunk = 3072;     // A ranges staged per chunk
+constexpr int kSpanMax = 384;     // B rows staged per sub-tile
+constexpr int kBMax = 768;        // B ranges staged per sub-tile
+constexpr int kBitWords = 6144;   // union bitmaps (PRE, SUF, BU) or direct windows
 constexpr int kStageMax = 6144;   // output entries staged per chunk
+constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
+constexpr int kRowWords = 6;      // row mode: 64-bit window words per thread (384 columns)
+constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
+constexpr int kSlot = 16;         // row mode: output entries kept per thread
 constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
 constexpr unsigned long long kFlag = 1ull << 63;
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-enum TileMode : int { kTiled = 0, kDirect = 1, kEmpty = 2 };
+enum TileMode : uint32_t { kTiled = 0, kDirect = 1, kEmpty = 2 };
 
 struct ChunkDesc {
   unsigned long long agg;       // kFlag | entries of the chunk
@@ -76,26 +81,52 @@ struct FusedArgs {
   uint32_t nrows;
   uint32_t chunk_rows;  // multiple of kSubRows, <= kChunkMax
   uint32_t nchunks;
+  uint32_t row_mode;    // 1: a thread per row (shared window); 0: tile-staged rows
+  uint32_t row_words;   // row mode: 64-bit window words used per thread (<= kRowWords)
+};
+
+// One staged B window: rows [bs, bf] and their ranges.
+struct BBuf {
+  uint64_t brow[kSpanMax + 1];
+  uint2 b[kBMax];
+};
+
+// A sub-tile's plan, made when its chunk starts.
+struct SubDesc {
+  uint32_t bs, bf;    // B rows named by the sub-tile's A ranges
+  uint32_t wmax;      // widest A range (rows)
+  uint32_t mode;      // TileMode
+  uint64_t b0, b1;    // B entries of rows bs..bf
+};
+
+struct TileBufs {
+  BBuf bb[2];                     // double-buffered B windows
+  uint32_t bits[kBitWords];
+  uint32_t stage[kStageMax];
 };
 
 struct Smem {
-  uint64_t arow[kSubRows + 1];
-  uint64_t brow[kSpanMax + 1];
-  uint2 a[kAMax];
-  uint2 b[kBMax];
-  uint32_t bits[kBitWords];
-  uint32_t stage[kStageMax];
+  uint32_t crow[kChunkMax + 1];   // chunk A row map, relative to its first entry
+  uint2 achunk[kAChunk];          // chunk A ranges
+  SubDesc sub[kSubMax];
+  union {
+    TileBufs t;
+  } u;
   uint32_t incl[kChunkMax];       // row entry counts, then their inclusive prefix
   uint32_t sub_off[kSubRows];     // stage offset of each row of the sub-tile
   unsigned long long red[kWarps];
-  uint32_t redu[2 * kWarps];
+  uint32_t redu[2][3 * kWarps];  // double-buffered block reductions
   unsigned long long prefix;
   uint32_t chunk;
   uint32_t stage_used;   // staged entries of the chunk
   uint32_t staged_rows;  // leading rows of the chunk whose runs are staged
   uint32_t stage_open;   // 0 once a row did not fit
   uint32_t sub_fit;      // rows of the current sub-tile that were staged
+  uint32_t a_staged;     // the chunk's A ranges are in achunk
 };
+
+// two CTAs per SM: 2 x (layout + 1 KB reserved) within the SM's 228 KB
+static_assert(2 * (sizeof(Smem) + 1024) <= 228 * 1024, "shared layout exceeds two CTAs per SM");
 
 // ---- small helpers -----------------------------------------------------------
 
@@ -106,40 +137,54 @@ __device__ __forceinline__ uint32_t word_mask(uint32_t rs, uint32_t re, uint64_t
   return (~0u << uint32_t(lo - c0)) & (~0u >> uint32_t(31 - (hi - c0)));
 }
 
-// Union of staged B row j on the word starting at c0.
-__device__ __forceinline__ uint32_t row_mask(const Smem& S, uint64_t b_base, uint32_t j, uint64_t c0) {
-  uint32_t k0 = uint32_t((S.brow[j] - b_base) >> 1), k1 = uint32_t((S.brow[j + 1] - b_base) >> 1);
+// Union of staged B row j (window-relative) on the word starting at c0.
+__device__ __forceinline__ uint32_t row_mask(const BBuf& B, uint64_t b_base, uint32_t j, uint64_t c0) {
+  uint32_t k0 = uint32_t((B.brow[j] - b_base) >> 1), k1 = uint32_t((B.brow[j + 1] - b_base) >> 1);
   uint32_t m = 0;
-  for (uint32_t k = k0; k < k1; ++k) m |= word_mask(S.b[k].x, S.b[k].y, c0);
+  for (uint32_t k = k0; k < k1; ++k) m |= word_mask(B.b[k].x, B.b[k].y, c0);
   return m;
 }
+
+// 8-byte asynchronous global -> shared copy (completes at cp.async.wait_group).
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+  const uint32_t d = uint32_t(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned runtime_group_mask(int g) {
   return g == 32 ? kFullMask : (((1u << g) - 1u) << (lane_id() & ~(g - 1)));
 }
 
-// Block-wide min and max of a uint32 pair (all threads receive both).
-__device__ void block_minmax(Smem& S, uint32_t& mn, uint32_t& mx) {
+// Block-wide (min a, max b, max c) with one barrier: warp partials go to one
+// of two buffers, alternating, so the next reduction cannot overwrite a
+// buffer that a slow warp is still reading.  All threads receive the result.
+__device__ void block_min_max_max(Smem& S, uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& phase) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    mn = min(mn, __shfl_xor_sync(kFullMask, mn, o));
-    mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
+    a = min(a, __shfl_xor_sync(kFullMask, a, o));
+    b = max(b, __shfl_xor_sync(kFullMask, b, o));
+    c = max(c, __shfl_xor_sync(kFullMask, c, o));
   }
+  uint32_t* buf = S.redu[phase & 1];
+  phase ^= 1;
   const int w = threadIdx.x >> 5;
-  __syncthreads();
   if ((threadIdx.x & 31) == 0) {
-    S.redu[w] = mn;
-    S.redu[kWarps + w] = mx;
+    buf[w] = a;
+    buf[kWarps + w] = b;
+    buf[2 * kWarps + w] = c;
   }
   __syncthreads();
-  mn = S.redu[0];
-  mx = S.redu[kWarps];
+  a = buf[0];
+  b = buf[kWarps];
+  c = buf[2 * kWarps];
 #pragma unroll
   for (int i = 1; i < kWarps; ++i) {
-    mn = min(mn, S.redu[i]);
-    mx = max(mx, S.redu[kWarps + i]);
+    a = min(a, buf[i]);
+    b = max(b, buf[kWarps + i]);
+    c = max(c, buf[2 * kWarps + i]);
   }
-  __syncthreads();
 }
 
 __device__ unsigned long long block_sum(Smem& S, unsigned long long v) {
@@ -168,32 +213,40 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
 // ---- tiled path ----------------------------------------------------------------
 
 struct TileGeom {
-  uint64_t a_base, b_base;
-  uint32_t bs;    // first staged B row
-  uint32_t span;  // staged B rows
-  uint64_t base;  // first column of the window (32-aligned)
-  uint32_t nwt;   // window words (the last one is always zero)
+  const BBuf* B;      // the staged B window
+  uint32_t r0;        // first chunk row of the sub-tile
+  uint64_t b_base;
+  uint32_t bs;        // first staged B row
+  uint32_t span;      // staged B rows
+  uint64_t base;      // first column of the window (32-aligned)
+  uint32_t nwt;       // window words (the last one is always zero)
   uint32_t sb_shift;  // union block rows = 1 << sb_shift
+  uint32_t pitch;     // words between two window words of PRE / SUF (odd)
+  uint32_t bpitch;    // the same for BU (odd)
 };
+
+// Union bitmaps are stored word-major -- PRE[w * pitch + j] -- with an odd
+// pitch, so lanes reading consecutive words of one row, or consecutive rows
+// of one word, hit distinct banks.
 
 // OR of the union bitmaps covering A row r (sub-tile local) on window word w.
 __device__ __forceinline__ uint32_t tiled_acc(const Smem& S, const TileGeom& T, uint32_t r, uint32_t w) {
-  const uint32_t* PRE = S.bits;
-  const uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
-  const uint32_t* BU = SUF + size_t(T.span) * T.nwt;
+  const uint32_t* PRE = S.u.t.bits + size_t(w) * T.pitch;
+  const uint32_t* SUF = S.u.t.bits + size_t(T.nwt) * T.pitch + size_t(w) * T.pitch;
+  const uint32_t* BU = S.u.t.bits + 2 * size_t(T.nwt) * T.pitch + size_t(w) * T.bpitch;
   const uint64_t c0 = T.base + 32ull * w;
-  const uint32_t k0 = uint32_t((S.arow[r] - T.a_base) >> 1), k1 = uint32_t((S.arow[r + 1] - T.a_base) >> 1);
+  const uint32_t k0 = S.crow[T.r0 + r] >> 1, k1 = S.crow[T.r0 + r + 1] >> 1;
   uint32_t acc = 0;
   for (uint32_t k = k0; k < k1; ++k) {
-    const uint2 ar = S.a[k];
+    const uint2 ar = S.achunk[k];
     if (ar.y < ar.x) continue;
     const uint32_t s = ar.x - T.bs, f = ar.y - T.bs;
     const uint32_t bS = s >> T.sb_shift, bF = f >> T.sb_shift;
     if (bS == bF) {
-      for (uint32_t j = s; j <= f; ++j) acc |= row_mask(S, T.b_base, j, c0);
+      for (uint32_t j = s; j <= f; ++j) acc |= row_mask(*T.B, T.b_base, j, c0);
     } else {
-      acc |= SUF[size_t(s) * T.nwt + w] | PRE[size_t(f) * T.nwt + w];
-      for (uint32_t bb = bS + 1; bb < bF; ++bb) acc |= BU[size_t(bb) * T.nwt + w];
+      acc |= SUF[s] | PRE[f];
+      for (uint32_t bb = bS + 1; bb < bF; ++bb) acc |= BU[bb];
     }
   }
   return acc;
@@ -249,7 +302,7 @@ __device__ uint32_t tiled_row(const Smem& S, const TileGeom& T, uint32_t r, int 
 
 template <class Emit>
 __device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row, uint32_t* bits, uint32_t* reach,
-                               unsigned long long* nnz_acc, Emit&& emit) {
+                               unsigned long long* nnz_acc, Emit&& emit, uint32_t ww = kDirectWW) {
   const int lg = lane_id();
   uint64_t a0, a1;
   if (a_identity) {
@@ -293,8 +346,8 @@ __device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row
   const uint64_t base = mn & ~31u;
   const uint64_t nw_total = ((uint64_t(mx) - base) >> 5) + 2;
   uint32_t carry = 0;
-  for (uint64_t w0 = 0; w0 < nw_total; w0 += kDirectWW) {
-    const uint32_t nwc = uint32_t(min(uint64_t(kDirectWW), nw_total - w0));
+  for (uint64_t w0 = 0; w0 < nw_total; w0 += ww) {
+    const uint32_t nwc = uint32_t(min(uint64_t(ww), nw_total - w0));
     const uint64_t cb = base + 32 * w0;
     const uint64_t ce = cb + 32ull * nwc - 1;
     for (uint32_t w = lg; w < nwc; w += 32) {
@@ -411,33 +464,487 @@ __device__ void lookback_warp(const FusedArgs& p, uint32_t t, unsigned long long
   prefix_nnz = pre_nnz;
 }
 
-// Warp 0: stage offsets for the sub-tile's rows [r0, r0 + rows) whose counts
-// are in S.incl; rows that fit are a prefix of the sub-tile.
+// Warp 0: stage offsets for the sub-tile's rows [r0, r0 + rows) (rows <= 64,
+// two consecutive rows per lane) whose counts are in S.incl; rows that fit
+// the staging area are a prefix of the sub-tile.
 __device__ void stage_rows(Smem& S, uint32_t r0, uint32_t rows) {
   const int lane = lane_id();
-  const uint32_t v = lane < int(rows) ? S.incl[r0 + lane] : 0u;
-  uint32_t incl = group_incl_sum<32>(kFullMask, v, lane);
-  const uint32_t used = S.stage_used;
+  const uint32_t ra = 2 * lane, rb = ra + 1;
+  const uint64_t va = ra < rows ? S.incl[r0 + ra] : 0u, vb = rb < rows ? S.incl[r0 + rb] : 0u;
+  const uint64_t pair = va + vb;
+  uint64_t inc = pair;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t u = __shfl_up_sync(kFullMask, inc, o);
+    if (lane >= o) inc += u;
+  }
+  const uint64_t ea = inc - pair, eb = ea + va;
+  const uint64_t used = S.stage_used;
   const bool open = S.stage_open != 0;
-  const bool fits = open && lane < int(rows) && uint64_t(used) + incl <= uint64_t(kStageMax);
-  const unsigned fit_mask = __ballot_sync(kFullMask, fits);
-  const uint32_t nfit = __popc(fit_mask);  // a prefix: incl grows with the lane
-  if (lane < int(rows)) S.sub_off[lane] = used + incl - v;
-  const uint32_t fit_total = nfit ? __shfl_sync(kFullMask, incl, int(nfit) - 1) : 0u;
+  const bool fa = open && ra < rows && used + ea + va <= uint64_t(kStageMax);
+  const bool fb = open && rb < rows && used + eb + vb <= uint64_t(kStageMax);
+  // the fitting rows are a prefix: their inclusive sums grow with the row
+  const uint32_t nfit = __popc(__ballot_sync(kFullMask, fa)) + __popc(__ballot_sync(kFullMask, fb));
+  if (ra < rows) S.sub_off[ra] = uint32_t(used + ea);
+  if (rb < rows) S.sub_off[rb] = uint32_t(used + eb);
+  uint64_t fit_end = fb ? eb + vb : (fa ? ea + va : 0u);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    uint64_t u = __shfl_xor_sync(kFullMask, fit_end, o);
+    fit_end = u > fit_end ? u : fit_end;
+  }
   __syncwarp();
   if (lane == 0) {
     S.sub_fit = nfit;
-    S.stage_used = used + fit_total;
+    S.stage_used = uint32_t(used + fit_end);
     if (nfit < rows) S.stage_open = 0;
     S.staged_rows += nfit;
   }
 }
 
+// ---- light path: one C row by one thread --------------------------------------
+//
+// For products whose rows union only a handful of B ranges (powers of A, the
+// final A^d * (A+I)^k product) a thread per row beats any cooperative scheme:
+// the row's ranges -- read from the staged chunk of A and from B through L1 --
+// are ORed into a 128-column register bitmap anchored at the row's first
+// column; the runs come out with the same boundary masks as the tiled gather,
+// on 64-bit words.  Rows wider than the window take further 128-column
+// windows, each re-reading the row's ranges.
+template <bool A_ID, class Emit>
+__device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const FusedArgs& p, uint32_t c0row,
+                              uint32_t r, bool a_staged, unsigned long long* nnz_acc, Emit&& emit) {
+  const uint64_t row = uint64_t(c0row) + r;
+  uint64_t a0, a1;
+  if (A_ID) {
+    a0 = 0;
+    a1 = 1;
+  } else if (a_staged) {
+    a0 = crow[r] >> 1;
+    a1 = crow[r + 1] >> 1;
+  } else {
+    a0 = p.a_rowmap[row] >> 1;
+    a1 = p.a_rowmap[row + 1] >> 1;
+  }
+  auto a_range = [&](uint64_t k) -> uint2 {
+    if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
+    return a_staged ? achunk[k] : load_range(p.a_entries, k);
+  };
+  // column band of the row
+  uint32_t lo = 0xffffffffu, hi = 0;
+  for (uint64_t k = a0; k < a1; ++k) {
+    const uint2 ar = a_range(k);
+    if (ar.y < ar.x) continue;
+    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    for (uint64_t t = t0; t < t1; ++t) {
+      const uint2 b = load_range(p.b_entries, t);
+      if (b.y < b.x) continue;
+      lo = min(lo, b.x);
+      hi = max(hi, b.y);
+    }
+  }
+  if (lo > hi) return 0;
+  uint32_t count = 0;
+  uint64_t carry = 0;
+  for (uint64_t wb = lo & ~63u; wb <= hi; wb += 128) {
+    uint64_t w0 = 0, w1 = 0;
+    for (uint64_t k = a0; k < a1; ++k) {
+      const uint2 ar = a_range(k);
+      if (ar.y < ar.x) continue;
+      const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+      for (uint64_t t = t0; t < t1; ++t) {
+        const uint2 b = load_range(p.b_entries, t);
+        const uint64_t x = max(uint64_t(b.x), wb), y = min(uint64_t(b.y), wb + 127);
+        if (b.y < b.x || x > y) continue;
+        const uint32_t xs = uint32_t(x - wb), ys = uint32_t(y - wb);
+        if (xs < 64) w0 |= (~0ull << xs) & (ys < 64 ? (~0ull >> (63 - ys)) : ~0ull);
+        if (ys >= 64) w1 |= (~0ull << (xs < 64 ? 0 : xs - 64)) & (~0ull >> (127 - ys));
+      }
+    }
+    if (nnz_acc) *nnz_acc += __popcll(w0) + __popcll(w1);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint64_t x = h ? w1 : w0;
+      const uint64_t sh = (x << 1) | carry;
+      uint64_t bnd = ((x ^ sh) & x) | (sh & ~x);
+      const uint64_t c0 = wb + 64 * h;
+      while (bnd) {
+        const int bit = __ffsll(bnd) - 1;
+        bnd &= bnd - 1;
+        emit(count, uint32_t(c0 + bit - (count & 1)));
+        ++count;
+      }
+      carry = x >> 63;
+    }
+  }
+  if (carry) {  // a run reaching the last window's end closes at column hi
+    emit(count, hi);
+    ++count;
+  }
+  return count;
+}
+
+// ---- row mode: one C row by one thread, bitvector window in shared memory ---
+//
+// The row kernel below keeps its shared footprint small (a window, a reach
+// entry per window word and an output slot per thread, plus the chunk's row
+// counts) so that most of the SM's L1 caches the B ranges the threads read:
+// the lanes of a warp take consecutive rows, whose B slices overlap, and
+// neighbouring warps cover neighbouring rows.
+//
+// A thread's window covers row_words x 64 columns anchored 64 columns below
+// the row's first B range.  A B range [x, y] costs O(1) whatever its length:
+// its two edge words are ORed and the full words between them are recorded
+// as a reach entry (the last full word + 1) at the first of them; a running
+// maximum over reach while gathering turns them into full words.  The runs
+// are gathered with 64-bit map01 / map10 boundary masks and ffs and appended
+// to the thread's output slot at position `pos`.  row_fast returns false,
+// leaving no trace in nnz, when a range falls outside the window or the runs
+// overflow the slot; the caller then takes the windowed register path.
+constexpr int kRowRowsPerThread = kChunkMax / kThreads;
+
+struct RowSmem {
+  uint64_t win[kRowWords * kThreads];   // word w of thread t at [w * kThreads + t]
+  uint16_t reach[kRowWords * kThreads];
+  uint32_t slot[kSlot * kThreads];
+  uint32_t incl[kChunkMax];
+  uint32_t slow[kSlowMax];              // rows left to the warp-cooperative path
+  unsigned long long red[kWarps];
+  unsigned long long prefix;
+  uint32_t chunk;
+  uint32_t nslow;
+};
+// the warp-cooperative path reuses the row windows: 32-bit bits + reach per warp
+constexpr int kRowDirectWW = int(sizeof(uint64_t) * kRowWords * kThreads / sizeof(uint32_t)) / (2 * kWarps);
+
+// base_hint: ~0 anchors the window 64 columns below the row's first B range;
+// any other value is the window's first column (a multiple of 64).
 template <bool A_ID>
-__global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
+__device__ bool row_fast(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
+                         unsigned long long& nnz, uint64_t base_hint) {
+  const int tid = threadIdx.x;
+  uint64_t* win = S.win + tid;
+  uint16_t* reach = S.reach + tid;
+  uint32_t* slot = S.slot + tid;
+  const uint32_t W = p.row_words;
+  uint64_t a0, a1;
+  if (A_ID) {
+    a0 = 0;
+    a1 = 1;
+  } else {
+    a0 = __ldg(p.a_rowmap + row) >> 1;
+    a1 = __ldg(p.a_rowmap + row + 1) >> 1;
+  }
+  for (uint32_t w = 0; w < W; ++w) {
+    win[w * kThreads] = 0;
+    reach[w * kThreads] = 0;
+  }
+  const uint64_t cols = 64ull * W;
+  uint64_t base = 0;
+  bool any = false;
+  uint32_t wtop = 0;
+  // the open run, kept in registers: ranges that overlap or touch it extend
+  // it; any other range first flushes it into the window
+  uint32_t run_lo = 0, run_hi = 0;
+  auto flush = [&](uint32_t x, uint32_t y) {
+    const uint32_t xs = uint32_t(x - base), ys = uint32_t(y - base);
+    const uint32_t ws = xs >> 6, we = ys >> 6;
+    const uint64_t lo = ~0ull << (xs & 63), hi = ~0ull >> (63 - (ys & 63));
+    if (ws == we) {
+      win[ws * kThreads] |= lo & hi;
+    } else {
+      win[ws * kThreads] |= lo;
+      win[we * kThreads] |= hi;
+      if (we > ws + 1) {
+        uint16_t& rr = reach[(ws + 1) * kThreads];
+        if (rr < we) rr = uint16_t(we);
+      }
+    }
+    wtop = max(wtop, we);
+  };
+  for (uint64_t k = a0; k < a1; ++k) {
+    const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
+    if (ar.y < ar.x) continue;
+    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    for (uint64_t t = t0; t < t1; ++t) {
+      const uint2 b = load_range(p.b_entries, t);
+      if (b.y < b.x) continue;
+      if (!any) {
+        any = true;
+        base = base_hint != ~0ull ? base_hint : (b.x >= 64 ? (uint64_t(b.x) & ~63ull) - 64 : 0);
+        run_lo = b.x;
+        run_hi = b.y;
+        continue;
+      }
+      if (uint64_t(b.x) <= uint64_t(run_hi) + 1 && uint64_t(b.y) + 1 >= run_lo) {
+        run_lo = min(run_lo, b.x);
+        run_hi = max(run_hi, b.y);
+        continue;
+      }
+      // merging may have carried the open run past the window: every flush
+      // checks the run it writes
+      if (run_lo < base || uint64_t(run_hi) >= base + cols) return false;
+      flush(run_lo, run_hi);
+      run_lo = b.x;
+      run_hi = b.y;
+    }
+  }
+  if (any) {
+    if (run_lo < base || uint64_t(run_hi) >= base + cols) return false;
+    flush(run_lo, run_hi);
+  }
+  count = 0;
+  if (!any) return true;
+  uint64_t carry = 0, n = 0;
+  uint32_t run = 0, c = 0;
+  for (uint32_t w = 0; w <= wtop; ++w) {
+    uint64_t x = win[w * kThreads];
+    run = max(run, uint32_t(reach[w * kThreads]));
+    if (run > w) x = ~0ull;
+    n += __popcll(x);
+    const uint64_t sh = (x << 1) | carry;
+    uint64_t bnd = ((x ^ sh) & x) | (sh & ~x);
+    while (bnd) {
+      const int bit = __ffsll(bnd) - 1;
+      bnd &= bnd - 1;
+      if (pos + c >= uint32_t(kSlot)) return false;
+      slot[(pos + c) * kThreads] = uint32_t(base + 64ull * w + bit - (c & 1));
+      ++c;
+    }
+    carry = x >> 63;
+  }
+  if (carry) {  // the run reaching the end of word wtop closes there
+    if (pos + c >= uint32_t(kSlot)) return false;
+    slot[(pos + c) * kThreads] = uint32_t(base + 64ull * wtop + 63);
+    ++c;
+  }
+  count = c;
+  nnz += n;
+  return true;
+}
+
+// Exact column band [lo, hi] of a C row (lo > hi when the row is empty).
+template <bool A_ID>
+__device__ void row_band(const FusedArgs& p, uint64_t row, uint32_t& lo, uint32_t& hi) {
+  uint64_t a0, a1;
+  if (A_ID) {
+    a0 = 0;
+    a1 = 1;
+  } else {
+    a0 = __ldg(p.a_rowmap + row) >> 1;
+    a1 = __ldg(p.a_rowmap + row + 1) >> 1;
+  }
+  lo = 0xffffffffu;
+  hi = 0;
+  for (uint64_t k = a0; k < a1; ++k) {
+    const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
+    if (ar.y < ar.x) continue;
+    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    for (uint64_t t = t0; t < t1; ++t) {
+      const uint2 b = load_range(p.b_entries, t);
+      if (b.y < b.x) continue;
+      lo = min(lo, b.x);
+      hi = max(hi, b.y);
+    }
+  }
+}
+
+// Fast path with one retry anchored at the row's exact band.
+template <bool A_ID>
+__device__ bool row_fast_retry(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
+                               unsigned long long& nnz) {
+  if (row_fast<A_ID>(S, p, row, pos, count, nnz, ~0ull)) return true;
+  uint32_t lo, hi;
+  row_band<A_ID>(p, row, lo, hi);
+  if (lo > hi) return false;
+  const uint64_t base = uint64_t(lo) & ~63ull;
+  if (uint64_t(hi) >= base + 64ull * p.row_words) return false;
+  return row_fast<A_ID>(S, p, row, pos, count, nnz, base);
+}
+
+// The row kernel: chunks from the ticket; thread (warp, lane) owns chunk rows
+// (warp * kRowRowsPerThread + u) * 32 + lane; counts, chunk prefix, look-back,
+// then every thread writes its rows from its slot (or recomputes them).
+template <bool A_ID>
+__global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RowSmem& S = *reinterpret_cast<RowSmem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* dbits = reinterpret_cast<uint32_t*>(S.win) + size_t(warp) * 2 * kRowDirectWW;
+  uint32_t* dreach = dbits + kRowDirectWW;
+  while (true) {
+    if (tid == 0) {
+      S.chunk = atomicAdd(p.ticket, 1u);
+      S.nslow = 0;
+    }
+    __syncthreads();
+    const uint32_t t = S.chunk;
+    if (t >= p.nchunks) break;
+    const uint32_t c0row = t * p.chunk_rows;
+    const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
+    unsigned long long nnz_acc = 0;
+    uint32_t fast_mask = 0, pos = 0;
+    // rows that miss the window wait for the warp-cooperative pass below, so
+    // one wide row never holds a whole chunk behind a single thread
+#pragma unroll
+    for (int u = 0; u < kRowRowsPerThread; ++u) {
+      const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
+      if (r < crows) {
+        uint32_t cnt = 0;
+        if (row_fast_retry<A_ID>(S, p, uint64_t(c0row) + r, pos, cnt, nnz_acc)) {
+          fast_mask |= 1u << u;
+          pos += cnt;
+        } else {
+          const uint32_t i = atomicAdd(&S.nslow, 1u);
+          if (i < uint32_t(kSlowMax)) {
+            S.slow[i] = r;
+          } else {
+            cnt = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
+          }
+          atomicAdd(&p.ctl->slow_rows, 1ull);
+        }
+        S.incl[r] = cnt;
+      }
+    }
+    __syncthreads();
+    const uint32_t nslow = min(S.nslow, uint32_t(kSlowMax));
+    for (uint32_t i = warp; i < nslow; i += kWarps) {
+      const uint32_t r = S.slow[i];
+      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
+                                    [](uint64_t, uint32_t) {}, kRowDirectWW);
+      if (lane == 0) S.incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+    }
+    __syncthreads();
+    // chunk prefix over the row counts (kRowRowsPerThread consecutive rows per thread)
+    {
+      uint32_t loc[kRowRowsPerThread];
+      uint64_t s = 0;
+#pragma unroll
+      for (int k = 0; k < kRowRowsPerThread; ++k) {
+        const uint32_t r = tid * kRowRowsPerThread + k;
+        s += r < crows ? S.incl[r] : 0u;
+        loc[k] = uint32_t(s);
+      }
+      uint64_t inc = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint64_t u = __shfl_up_sync(kFullMask, inc, o);
+        if (lane >= o) inc += u;
+      }
+      if (lane == 31) S.red[warp] = inc;
+      __syncthreads();
+      uint64_t wpre = 0;
+      for (int i = 0; i < warp; ++i) wpre += S.red[i];
+      const uint64_t excl = wpre + inc - s;
+      if (excl + s > 0xffffffffull) atomicOr(&p.ctl->status, 16ull);
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kRowRowsPerThread; ++k) {
+        const uint32_t r = tid * kRowRowsPerThread + k;
+        if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
+      }
+    }
+    // chunk nnz
+    unsigned long long v = nnz_acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+    if (lane == 0) S.red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long chunk_nnz = 0;
+      for (int i = 0; i < kWarps; ++i) chunk_nnz += S.red[i];
+      const unsigned long long chunk_cnt = S.incl[crows - 1];
+      unsigned long long pre, pre_nnz;
+      lookback_warp(p, t, chunk_cnt, chunk_nnz, pre, pre_nnz);
+      if (lane == 0) {
+        S.prefix = pre;
+        if (t == p.nchunks - 1) {
+          p.ctl->total = pre + chunk_cnt;
+          p.ctl->nnz = pre_nnz + chunk_nnz;
+          if (pre + chunk_cnt > p.cap) p.ctl->overflow = pre + chunk_cnt;
+        }
+      }
+    }
+    __syncthreads();
+    const unsigned long long prefix = S.prefix;
+    for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
+    if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
+    pos = 0;
+#pragma unroll
+    for (int u = 0; u < kRowRowsPerThread; ++u) {
+      const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
+      if (r >= crows) continue;
+      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+      const bool fast = (fast_mask >> u) & 1u;
+      if (n && dst + n > p.cap) {
+        atomicOr(&p.ctl->overflow, 1ull);
+      } else if (fast) {
+        for (uint32_t k = 0; k < n; ++k) p.c_entries[dst + k] = S.slot[(pos + k) * kThreads + tid];
+      }
+      if (fast) pos += n;
+    }
+    // rows that missed the window: the listed ones by warps, any overflow of
+    // the list by its own thread
+    for (uint32_t i = warp; i < nslow; i += kWarps) {
+      const uint32_t r = S.slow[i];
+      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+      if (n == 0 || dst + n > p.cap) continue;
+      uint32_t* out = p.c_entries + dst;
+      bool bad = false;
+      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
+                                    [&](uint64_t k, uint32_t v) {
+                                      if (k < n) out[k] = v;
+                                      else bad = true;
+                                    },
+                                    kRowDirectWW);
+      if (bad || c != n) atomicOr(&p.ctl->status, 8ull);
+    }
+    if (S.nslow > uint32_t(kSlowMax)) {
+#pragma unroll
+      for (int u = 0; u < kRowRowsPerThread; ++u) {
+        const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
+        if (r >= crows || ((fast_mask >> u) & 1u)) continue;
+        bool listed = false;
+        for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
+        if (listed) continue;
+        const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+        const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+        if (n == 0 || dst + n > p.cap) continue;
+        uint32_t* out = p.c_entries + dst;
+        uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr, [&](uint64_t k, uint32_t v) {
+          if (k < n) out[k] = v;
+        });
+        if (c != n) atomicOr(&p.ctl->status, 8ull);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Issues the asynchronous copies of sub-tile q's B window into its buffer
+// and commits them as one group (an empty group when q stages nothing).
+__device__ __forceinline__ void prefetch_window(Smem& S, const FusedArgs& p, uint32_t q, uint32_t nsub) {
+  if (q < nsub && S.sub[q].mode == kTiled) {
+    const SubDesc d = S.sub[q];
+    BBuf& B = S.u.t.bb[q & 1];
+    const uint32_t span = d.bf - d.bs + 1;
+    for (uint32_t k = threadIdx.x; k <= span; k += kThreads) cp_async8(&B.brow[k], p.b_rowmap + d.bs + k);
+    const uint64_t r0 = d.b0 >> 1;
+    const uint32_t nr = uint32_t((d.b1 - d.b0) >> 1);
+    for (uint32_t k = threadIdx.x; k < nr; k += kThreads)
+      cp_async8(&B.b[k], reinterpret_cast<const uint2*>(p.b_entries) + r0 + k);
+  }
+  cp_async_commit();
+}
+
+template <bool A_ID>
+__global__ void __launch_bounds__(kThreads, 2) k_spgemm_fused(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t phase = 0;  // reduction buffer parity (uniform over the CTA)
 
   while (true) {
     if (tid == 0) {
@@ -451,130 +958,152 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
     if (t >= p.nchunks) break;
     const uint32_t c0row = t * p.chunk_rows;
     const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
+    const uint32_t nsub = (crows + kSubRows - 1) / kSubRows;
     unsigned long long nnz_acc = 0;
     bool any_direct = false;
 
-    for (uint32_t r0 = 0; r0 < crows; r0 += kSubRows) {
+    // ---- chunk plan: A row map and ranges once, then every sub-tile's B
+    // rows and B entry window, so sub-tile staging needs no further lookups
+    if (A_ID) {
+      for (uint32_t k = tid; k <= crows; k += kThreads) S.crow[k] = 2 * k;
+      if (tid == 0) S.a_staged = 1;
+    } else {
+      const uint64_t abase = p.a_rowmap[c0row];
+      const uint64_t aend = p.a_rowmap[c0row + crows];
+      const bool fits = ((aend - abase) >> 1) <= kAChunk;
+      if (fits)
+        for (uint32_t k = tid; k <= crows; k += kThreads) S.crow[k] = uint32_t(p.a_rowmap[c0row + k] - abase);
+      if (tid == 0) S.a_staged = fits ? 1u : 0u;
+    }
+    __syncthreads();
+    const bool a_staged = S.a_staged != 0;
+    if (a_staged) {
+      const uint64_t abase = A_ID ? 0 : p.a_rowmap[c0row];
+      for (uint32_t q = warp; q < nsub; q += kWarps) {
+        const uint32_t rq0 = q * kSubRows, rq1 = min(crows, rq0 + kSubRows);
+        const uint32_t k0 = S.crow[rq0] >> 1, k1 = S.crow[rq1] >> 1;
+        uint32_t mn = 0xffffffffu, mx = 0, wmax = 0;
+        for (uint32_t k = k0 + lane; k < k1; k += 32) {
+          uint2 r;
+          if (A_ID) {
+            r = make_uint2(c0row + k, c0row + k);
+          } else {
+            r = load_range(p.a_entries, (abase >> 1) + k);
+          }
+          S.achunk[k] = r;
+          if (r.y >= r.x) {
+            mn = min(mn, r.x);
+            mx = max(mx, r.y);
+            wmax = max(wmax, r.y - r.x + 1);
+          }
+        }
+        mn = group_min<32>(kFullMask, mn);
+        mx = group_max<32>(kFullMask, mx);
+        wmax = group_max<32>(kFullMask, wmax);
+        if (lane == 0) {
+          SubDesc d{};
+          d.bs = mn;
+          d.bf = mx;
+          d.wmax = wmax;
+          d.mode = mn > mx ? kEmpty : (mx - mn + 1 > uint32_t(kSpanMax) ? kDirect : kTiled);
+          S.sub[q] = d;
+        }
+      }
+    } else {
+      for (uint32_t q = tid; q < nsub; q += kThreads) S.sub[q].mode = kDirect;
+    }
+    __syncthreads();
+    for (uint32_t q = tid; q < nsub; q += kThreads) {
+      SubDesc& d = S.sub[q];
+      if (d.mode == kTiled) {
+        d.b0 = p.b_rowmap[d.bs];
+        d.b1 = p.b_rowmap[uint64_t(d.bf) + 1];
+        if (d.b1 < d.b0 || ((d.b1 - d.b0) >> 1) > uint64_t(kBMax)) d.mode = kDirect;
+      }
+    }
+    __syncthreads();
+    prefetch_window(S, p, 0, nsub);
+
+    for (uint32_t q = 0; q < nsub; ++q) {
+      const uint32_t r0 = q * kSubRows;
       const uint32_t i0 = c0row + r0;
       const uint32_t rows = min(uint32_t(kSubRows), crows - r0);
-      int mode = kTiled;
+      prefetch_window(S, p, q + 1, nsub);  // overlaps this sub-tile's work
+      cp_async_wait_prev();                 // this sub-tile's window has landed
+      __syncthreads();
+      const SubDesc d = S.sub[q];
+      uint32_t mode = d.mode;
       TileGeom T{};
 
-      // 1. A sub-tile
-      uint64_t a_cnt;
-      if (A_ID) {
-        if (tid <= int(rows)) S.arow[tid] = 2ull * tid;
-        if (tid < int(rows)) S.a[tid] = make_uint2(i0 + tid, i0 + tid);
-        T.a_base = 0;
-        a_cnt = rows;
-        __syncthreads();
-      } else {
-        if (tid <= int(rows)) S.arow[tid] = p.a_rowmap[i0 + tid];
-        __syncthreads();
-        T.a_base = S.arow[0];
-        a_cnt = (S.arow[rows] - T.a_base) >> 1;
-        if (a_cnt > kAMax) {
-          mode = kDirect;
-        } else {
-          for (uint32_t k = tid; k < a_cnt; k += kThreads) S.a[k] = load_range(p.a_entries, (T.a_base >> 1) + k);
-        }
-        __syncthreads();
-      }
-
-      // 2. B rows named by the sub-tile, and its column window
       if (mode == kTiled) {
-        uint32_t mn = 0xffffffffu, mx = 0;
-        for (uint32_t k = tid; k < a_cnt; k += kThreads) {
-          uint2 r = S.a[k];
+        // the sub-tile's column window over its staged B ranges
+        const BBuf& B = S.u.t.bb[q & 1];
+        T.B = &B;
+        T.r0 = r0;
+        T.bs = d.bs;
+        T.span = d.bf - d.bs + 1;
+        T.b_base = d.b0;
+        const uint32_t nb = uint32_t((d.b1 - d.b0) >> 1);
+        uint32_t mn = 0xffffffffu, mx = 0, unused = 0;
+        for (uint32_t k = tid; k < nb; k += kThreads) {
+          const uint2 r = B.b[k];
           if (r.y >= r.x) {
             mn = min(mn, r.x);
             mx = max(mx, r.y);
           }
         }
-        block_minmax(S, mn, mx);
+        block_min_max_max(S, mn, mx, unused, phase);
         if (mn > mx) {
           mode = kEmpty;
         } else {
-          T.bs = mn;
-          T.span = mx - mn + 1;
-          if (T.span > kSpanMax) mode = kDirect;
+          uint32_t sb = 2;
+          while (sb < kMaxBlock && sb * 4 <= d.wmax) sb <<= 1;
+          T.sb_shift = __ffs(sb) - 1;
+          T.base = mn & ~31u;
+          T.nwt = uint32_t(((uint64_t(mx) - T.base) >> 5) + 2);
+          T.pitch = T.span | 1u;
+          const uint32_t nblk = (T.span + sb - 1) >> T.sb_shift;
+          T.bpitch = nblk | 1u;
+          if ((2ull * T.pitch + T.bpitch) * T.nwt > kBitWords) mode = kDirect;
         }
       }
+
       if (mode == kTiled) {
-        for (uint32_t k = tid; k <= T.span; k += kThreads) S.brow[k] = p.b_rowmap[uint64_t(T.bs) + k];
-        __syncthreads();
-        T.b_base = S.brow[0];
-        const uint64_t b_cnt = (S.brow[T.span] - T.b_base) >> 1;
-        if (b_cnt > kBMax) {
-          mode = kDirect;
-        } else {
-          for (uint32_t k = tid; k < b_cnt; k += kThreads) S.b[k] = load_range(p.b_entries, (T.b_base >> 1) + k);
-        }
-        __syncthreads();
-        if (mode == kTiled) {
-          uint32_t mn = 0xffffffffu, mx = 0;
-          for (uint32_t k = tid; k < b_cnt; k += kThreads) {
-            uint2 r = S.b[k];
-            if (r.y >= r.x) {
-              mn = min(mn, r.x);
-              mx = max(mx, r.y);
+        // union bitmaps, one warp per (word, 32 staged rows): lane l holds
+        // R_j (j = 32 u + l) on word w; segmented OR-scans of width sb give
+        // the prefix (PRE) and suffix (SUF) unions inside each block; the
+        // block's last lane holds the block union (BU).
+        const BBuf& B = *T.B;
+        uint32_t* PRE = S.u.t.bits;
+        uint32_t* SUF = S.u.t.bits + size_t(T.nwt) * T.pitch;
+        uint32_t* BU = S.u.t.bits + 2 * size_t(T.nwt) * T.pitch;
+        const int sb = 1 << T.sb_shift;
+        const int ls = lane & (sb - 1);
+        const uint32_t nq = (T.span + 31) >> 5;
+        for (uint32_t task = warp; task < nq * T.nwt; task += kWarps) {
+          const uint32_t w = task / nq, u = task - w * nq;
+          const uint32_t j = (u << 5) + lane;
+          const uint32_t x = j < T.span ? row_mask(B, T.b_base, j, T.base + 32ull * w) : 0u;
+          uint32_t pre = x, suf = x;
+#pragma unroll
+          for (int o = 1; o < kMaxBlock; o <<= 1) {
+            if (o < sb) {
+              uint32_t pu = __shfl_up_sync(kFullMask, pre, o, sb);
+              if (ls >= o) pre |= pu;
+              uint32_t sv = __shfl_down_sync(kFullMask, suf, o, sb);
+              if (ls + o < sb) suf |= sv;
             }
           }
-          uint32_t wmax = 0;  // widest A range (rows)
-          for (uint32_t k = tid; k < a_cnt; k += kThreads) {
-            uint2 r = S.a[k];
-            if (r.y >= r.x) wmax = max(wmax, r.y - r.x + 1);
+          if (j < T.span) {
+            PRE[size_t(w) * T.pitch + j] = pre;
+            SUF[size_t(w) * T.pitch + j] = suf;
           }
-          block_minmax(S, mn, mx);
-          uint32_t zero = 0;
-          block_minmax(S, zero, wmax);
-          if (mn > mx) {
-            mode = kEmpty;
-          } else {
-            T.base = mn & ~31u;
-            T.nwt = uint32_t(((uint64_t(mx) - T.base) >> 5) + 2);
-            // union block: about a quarter of the widest A range, 2..64 rows
-            uint32_t sb = 2;
-            while (sb < 64 && sb * 4 <= wmax) sb <<= 1;
-            T.sb_shift = __ffs(sb) - 1;
-            const uint64_t nblk = (T.span + sb - 1) >> T.sb_shift;
-            if ((2ull * T.span + nblk) * T.nwt > kBitWords) mode = kDirect;
-          }
-        }
-      }
-
-      if (mode == kTiled) {
-        // 3. union bitmaps: R_j into PRE, then SUF (from R) and PRE (in place)
-        uint32_t* PRE = S.bits;
-        uint32_t* SUF = PRE + size_t(T.span) * T.nwt;
-        uint32_t* BU = SUF + size_t(T.span) * T.nwt;
-        const uint32_t items = T.span * T.nwt;
-        for (uint32_t it = tid; it < items; it += kThreads) {
-          const uint32_t j = it / T.nwt, w = it - j * T.nwt;
-          PRE[it] = row_mask(S, T.b_base, j, T.base + 32ull * w);
-        }
-        __syncthreads();
-        const uint32_t sb = 1u << T.sb_shift;
-        const uint32_t nblk = (T.span + sb - 1) >> T.sb_shift;
-        for (uint32_t it = tid; it < nblk * T.nwt; it += kThreads) {
-          const uint32_t bb = it / T.nwt, w = it - bb * T.nwt;
-          const uint32_t j0 = bb << T.sb_shift, j1 = min(T.span, j0 + sb);
-          uint32_t acc = 0;
-          for (uint32_t j = j1; j-- > j0;) {
-            acc |= PRE[size_t(j) * T.nwt + w];
-            SUF[size_t(j) * T.nwt + w] = acc;
-          }
-          acc = 0;
-          for (uint32_t j = j0; j < j1; ++j) {
-            acc |= PRE[size_t(j) * T.nwt + w];
-            PRE[size_t(j) * T.nwt + w] = acc;
-          }
-          BU[size_t(bb) * T.nwt + w] = acc;
+          if (ls == sb - 1 && (j >> T.sb_shift) < T.bpitch) BU[size_t(w) * T.bpitch + (j >> T.sb_shift)] = pre;
         }
         __syncthreads();
 
-        // 4. rows: groups of g lanes, one window word per lane and chunk.
-        // A group holds at most 4 rows (g >= 4 lanes -> >= 8 groups).
+        // rows: groups of g lanes, one window word per lane and chunk; a
+        // group holds at most 4 rows (64 rows, >= 16 groups)
         const int g = T.nwt <= 4 ? 4 : T.nwt <= 8 ? 8 : T.nwt <= 16 ? 16 : 32;
         const int lg = tid & (g - 1);
         const unsigned gm = runtime_group_mask(g);
@@ -582,15 +1111,15 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
         const bool one_chunk = T.nwt <= uint32_t(g);
         uint32_t xs[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const uint32_t r = gid + q * ngroups;
-          xs[q] = 0;
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t r = gid + u * ngroups;
+          xs[u] = 0;
           if (r < rows) {
             uint32_t cnt;
             if (one_chunk) {
               const bool valid = uint32_t(lg) < T.nwt;
               const uint32_t x = valid ? tiled_acc(S, T, r, lg) : 0u;
-              xs[q] = x;
+              xs[u] = x;
               nnz_acc += __popc(x);
               uint32_t carry = 0;
               cnt = gather_chunk(x, valid, 0, g, lg, gm, carry, 0, T.nwt - 1, [](uint64_t, uint32_t) {});
@@ -605,24 +1134,23 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
         __syncthreads();
         const uint32_t fit = S.sub_fit;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const uint32_t r = gid + q * ngroups;
+        for (int u = 0; u < 4; ++u) {
+          const uint32_t r = gid + u * ngroups;
           if (r < fit) {
-            uint32_t* st = S.stage + S.sub_off[r];
+            uint32_t* st = S.u.t.stage + S.sub_off[r];
             if (one_chunk) {
               const bool valid = uint32_t(lg) < T.nwt;
               uint32_t carry = 0;
-              gather_chunk(xs[q], valid, T.base + 32ull * lg, g, lg, gm, carry, 0, T.nwt - 1,
+              gather_chunk(xs[u], valid, T.base + 32ull * lg, g, lg, gm, carry, 0, T.nwt - 1,
                            [&](uint64_t k, uint32_t v) { st[k] = v; });
             } else {
               tiled_row(S, T, r, g, lg, gm, nullptr, [&](uint64_t k, uint32_t v) { st[k] = v; });
             }
           }
         }
-        __syncthreads();
       } else if (mode == kDirect) {
         any_direct = true;
-        uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
+        uint32_t* bits = S.u.t.bits + size_t(warp) * 2 * kDirectWW;
         uint32_t* reach = bits + kDirectWW;
         for (uint32_t r = warp; r < rows; r += kWarps) {
           uint64_t c = direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, &nnz_acc, [](uint64_t, uint32_t) {});
@@ -633,29 +1161,28 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
         __syncthreads();
         const uint32_t fit = S.sub_fit;
         for (uint32_t r = warp; r < fit; r += kWarps) {
-          uint32_t* st = S.stage + S.sub_off[r];
+          uint32_t* st = S.u.t.stage + S.sub_off[r];
           direct_row(p, A_ID, uint64_t(i0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) { st[k] = v; });
         }
-        __syncthreads();
       } else {
         if (tid < int(rows)) S.incl[r0 + tid] = 0;
         __syncthreads();
         if (warp == 0) stage_rows(S, r0, rows);
-        __syncthreads();
       }
+      __syncthreads();
     }
 
-    // 5. chunk prefix over the row counts (8 consecutive rows per thread)
+    // ---- chunk prefix over the row counts (4 consecutive rows per thread)
     {
-      uint32_t loc[8];
+      constexpr int kPer = kChunkMax / kThreads;
+      uint32_t loc[kPer];
       uint64_t s = 0;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const uint32_t r = tid * 8 + k;
+      for (int k = 0; k < kPer; ++k) {
+        const uint32_t r = tid * kPer + k;
         s += r < crows ? S.incl[r] : 0u;
         loc[k] = uint32_t(s);
       }
-      // block exclusive scan of the per-thread sums
       uint64_t inc = s;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -669,8 +1196,8 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
       const uint64_t excl = wpre + inc - s;
       if (excl + s > 0xffffffffull) atomicOr(&p.ctl->status, 16ull);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const uint32_t r = tid * 8 + k;
+      for (int k = 0; k < kPer; ++k) {
+        const uint32_t r = tid * kPer + k;
         if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
       }
       __syncthreads();
@@ -693,18 +1220,18 @@ __global__ void __launch_bounds__(kThreads) k_spgemm_fused(FusedArgs p) {
     __syncthreads();
     const unsigned long long prefix = S.prefix;
 
-    // 6. rowmap, staged entries, and the rows that did not fit the stage
+    // ---- rowmap, staged entries, and the rows that did not fit the stage
     for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
     if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
     const uint32_t staged = S.stage_used;
     if (prefix + staged <= p.cap) {
-      for (uint32_t k = tid; k < staged; k += kThreads) p.c_entries[prefix + k] = S.stage[k];
+      for (uint32_t k = tid; k < staged; k += kThreads) p.c_entries[prefix + k] = S.u.t.stage[k];
     } else if (tid == 0) {
       atomicOr(&p.ctl->overflow, 1ull);
     }
     const uint32_t srows = S.staged_rows;
     if (srows < crows) {
-      uint32_t* bits = S.bits + size_t(warp) * 2 * kDirectWW;
+      uint32_t* bits = S.u.t.bits + size_t(warp) * 2 * kDirectWW;
       uint32_t* reach = bits + kDirectWW;
       for (uint32_t r = srows + warp; r < crows; r += kWarps) {
         const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
@@ -733,8 +1260,11 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
                          uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   if (n == 0) return;
-  auto kern = a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>;
-  const int smem = int(sizeof(Smem));
+  // row mode unless the tiled mode is requested
+  const bool row_mode = ctx->opt_spgemm_mode != 1;
+  auto kern = row_mode ? (a_identity ? k_spgemm_rowmode<true> : k_spgemm_rowmode<false>)
+                       : (a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>);
+  const int smem = int(row_mode ? sizeof(RowSmem) : sizeof(Smem));
   DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
   DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
@@ -772,6 +1302,9 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
   p.nrows = n;
   p.chunk_rows = chunk_rows;
   p.nchunks = nchunks;
+  p.row_mode = row_mode ? 1u : 0u;
+  p.row_words = kRowWords;
+  if (row_mode) ctx->stats.spgemm_light++;
   const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
   kern<<<grid, kThreads, smem, ctx->stream>>>(p);
   DVG_CUDA(cudaGetLastError());
@@ -930,6 +1463,8 @@ extern "C" dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncol
     p.nrows = a_nrows;
     p.chunk_rows = chunk_rows;
     p.nchunks = nchunks;
+    p.row_mode = 0;
+    p.row_words = kRowWords;
     const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
     kern<<<grid, kThreads, smem, stream>>>(p);
     DVG_CUDA(cudaGetLastError());

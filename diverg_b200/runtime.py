@@ -47,6 +47,10 @@ class Context:
     def set_option(self, key, value):
         N.check(N.lib().dvg_set_option(self.handle, key.encode(), int(value)))
 
+    def trim(self):
+        """Return the device memory cached by the context to CUDA."""
+        N.check(N.lib().dvg_trim(self.handle))
+
     def stats(self):
         s = N.DvgStats()
         N.check(N.lib().dvg_get_stats(self.handle, ctypes.byref(s)))

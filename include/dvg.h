@@ -63,6 +63,10 @@ typedef struct dvg_stats {
   uint64_t spadd_ns;            /* SpAdd passes */
   uint64_t spgemm_direct_tiles; /* SpGEMM row tiles that missed the staged path */
   uint64_t spgemm_reruns;       /* SpGEMMs re-run after an output capacity overflow */
+  uint64_t spgemm_light;        /* SpGEMMs run in the thread-per-row mode */
+  uint64_t spgemm_slow_rows;    /* thread-per-row rows that took the windowed fallback */
+  uint64_t host_alloc_ns;       /* host time spent in device allocation calls */
+  uint64_t host_sync_ns;        /* host time spent waiting on stream synchronisation */
 } dvg_stats;
 
 /* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /
@@ -83,8 +87,14 @@ dvg_status dvg_synchronize(dvg_context* ctx);
  * autotune, or 4/8/16/32 lanes per output row), "window_words" (two-pass path:
  * 0 = default, else 32-bit accumulator words per row group), "chunk_rows"
  * (fused path: 0 = automatic, else rows per output chunk, a multiple of 32 up
- * to 2048), "timing" (1 = time kernels with CUDA events into dvg_stats). */
+ * to 2048), "spgemm_mode" (fused path: 0 = automatic, 1 = tile-staged rows,
+ * 2 = a thread per row), "dindex_schedule" (0 = sum of powers of A, the
+ * default; 1 = the reference's squaring of A + I; both give the same index),
+ * "timing" (1 = time kernels with CUDA events into dvg_stats). */
 dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value);
+/* Device memory freed by the context's operations is kept for reuse; this
+ * returns all of it to the CUDA allocator. */
+dvg_status dvg_trim(dvg_context* ctx);
 dvg_status dvg_get_stats(const dvg_context* ctx, dvg_stats* out);
 dvg_status dvg_stats_reset(dvg_context* ctx);
 const char* dvg_last_error(void);

@@ -10,11 +10,13 @@ from tests.conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-# (algo, group lanes, window words): the fused tile-staged kernel, then the
-# two-pass row-direct kernel at "auto", every group size at its default
-# window, and tiny windows that force its multi-chunk path
-PLANS = [(0, 0, 0), (1, 0, 0), (1, 4, 0), (1, 8, 0), (1, 16, 0), (1, 32, 0), (1, 4, 1), (1, 8, 3), (1, 32, 2),
-         (1, 16, 37)]
+# (algo, group lanes, window words[, fused mode]): the fused kernel in its
+# automatic (thread per row), tile-staged and thread-per-row modes, then the two-pass
+# row-direct kernel at "auto", every group size at its default window, and
+# tiny windows that force its multi-chunk path
+FUSED = [(0, 0, 0, 0), (0, 0, 0, 1), (0, 0, 0, 2)]
+PLANS = FUSED + [(1, 0, 0), (1, 4, 0), (1, 8, 0), (1, 16, 0), (1, 32, 0), (1, 4, 1), (1, 8, 3), (1, 32, 2),
+                 (1, 16, 37)]
 
 
 @pytest.fixture(scope="module")
@@ -28,6 +30,7 @@ def set_plan(ctx, plan, chunk_rows=0):
     ctx.set_option("algo", plan[0])
     ctx.set_option("group_lanes", plan[1])
     ctx.set_option("window_words", plan[2])
+    ctx.set_option("spgemm_mode", plan[3] if len(plan) > 3 else 0)
     ctx.set_option("chunk_rows", chunk_rows)
 
 
@@ -58,7 +61,7 @@ def test_hbitvector_known_answer(ctx, plan):
 
 
 @pytest.mark.parametrize("name", ["x", "multi", "m"])
-@pytest.mark.parametrize("plan", [(0, 0, 0), (1, 0, 0), (1, 4, 0), (1, 32, 0), (1, 8, 3)])
+@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0), (1, 4, 0), (1, 32, 0), (1, 8, 3)])
 def test_gfa_fixture_products(ctx, name, plan):
     set_plan(ctx, plan)
     g = load_golden(f"gfa_{name}.npz")
@@ -88,7 +91,7 @@ def test_random_spgemm_reference_shape(ctx, plan):
     assert_same(ctx.spgemm(da, da).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", [(0, 0, 0), (1, 0, 0), (1, 4, 0), (1, 16, 0), (1, 8, 5)])
+@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0), (1, 4, 0), (1, 16, 0), (1, 8, 5)])
 def test_random_power_reference_shape(ctx, plan):
     # test_range_sparse.cpp:590-594: N = 6521, NNZ = 4000, K = 100
     set_plan(ctx, plan)
@@ -106,9 +109,9 @@ def test_random_spadd_reference_shapes(ctx, n, nnz):
     assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("algo", [0, 1])
-def test_rectangular_spgemm(ctx, algo):
-    set_plan(ctx, (algo, 0, 0))
+@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0)])
+def test_rectangular_spgemm(ctx, plan):
+    set_plan(ctx, plan)
     a = gen.random_matrix(3000, 30000, seed=5)
     b = gen.banded(3000, 64, 3.0, 16.0, seed=6)
     # a: 3000 x 3000, b: 3000 x 3000 -> check A*B and B*A
@@ -117,7 +120,7 @@ def test_rectangular_spgemm(ctx, algo):
         assert_same(ctx.spgemm(ctx.upload(x), ctx.upload(y)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", [(0, 0, 0), (1, 0, 0), (1, 8, 0), (1, 32, 4)])
+@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0), (1, 8, 0), (1, 32, 4)])
 def test_banded_spgemm(ctx, plan):
     set_plan(ctx, plan)
     a = gen.banded(1 << 16, 512, 4.0, 32.0, seed=31)
@@ -128,19 +131,24 @@ def test_banded_spgemm(ctx, plan):
     assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("algo,chunk_rows", [(0, 0), (0, 2048), (1, 0)])
-@pytest.mark.parametrize("window", [(100, 300), (0, 250), (150, 450), (1, 1), (7, 7), (0, 1)])
-def test_small_graph_index(ctx, window, algo, chunk_rows):
-    set_plan(ctx, (algo, 0, 0), chunk_rows)
+@pytest.mark.parametrize("plan,chunk_rows", [((0, 0, 0, 0), 0), ((0, 0, 0, 0), 2048), ((0, 0, 0, 1), 0),
+                                             ((0, 0, 0, 2), 0), ((0, 0, 0, 2), 2048), ((1, 0, 0), 0)])
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("window", [(100, 300), (0, 250), (150, 450), (1, 1), (7, 7), (0, 1), (3, 37), (0, 200)])
+def test_small_graph_index(ctx, window, plan, chunk_rows, schedule):
+    set_plan(ctx, plan, chunk_rows)
+    ctx.set_option("dindex_schedule", schedule)
     a, _ = gen.graph_adjacency(gen.small_graph_spec(100_000, seed=42))
     want = orc.dindex(omat(a), window[0], window[1], algo="hbv")
     got = ctx.distance_index(ctx.upload(a), *window).download()
     assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
 
 
-@pytest.mark.parametrize("algo", [0, 1])
-def test_graph_with_structural_bubbles_index(ctx, algo):
-    set_plan(ctx, (algo, 0, 0))
+@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0)])
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_graph_with_structural_bubbles_index(ctx, plan, schedule):
+    set_plan(ctx, plan)
+    ctx.set_option("dindex_schedule", schedule)
     spec = gen.GraphSpec(60_000, 1e-3, 2e-4, 0.5, 1, 50, 4.0, 0.05, 100, 2000, seed=8)
     a, st = gen.graph_adjacency(spec)
     assert st["n_sv"] > 0
@@ -162,9 +170,9 @@ def test_fused_tiled_single_chunk_and_stage_overflow(ctx, chunk_rows):
     # narrow band, many short output runs: staged sub-tiles; with large chunks
     # the output outgrows the staging area and the remaining rows are
     # recomputed into global memory
-    set_plan(ctx, (0, 0, 0), chunk_rows)
-    a = gen.banded(20_000, 20, 3.0, 1.0, seed=41)
-    b = gen.banded(20_000, 300, 10.0, 1.0, seed=42)
+    set_plan(ctx, (0, 0, 0, 1), chunk_rows)
+    a = gen.banded(20_000, 20, 1.2, 2.0, seed=41)
+    b = gen.banded(20_000, 300, 6.0, 1.0, seed=42)
     st = spgemm_case(ctx, a, b)
     assert st["spgemm_direct_tiles"] == 0
 
@@ -172,9 +180,9 @@ def test_fused_tiled_single_chunk_and_stage_overflow(ctx, chunk_rows):
 @pytest.mark.parametrize("chunk_rows", [0, 2048])
 def test_fused_tiled_multi_chunk(ctx, chunk_rows):
     # a sub-tile window wider than 32 words: lane groups loop over window chunks
-    set_plan(ctx, (0, 0, 0), chunk_rows)
-    a = gen.banded(20_000, 20, 3.0, 1.0, seed=43)
-    b = gen.banded(20_000, 500, 6.0, 1.0, seed=44)
+    set_plan(ctx, (0, 0, 0, 1), chunk_rows)
+    a = gen.banded(20_000, 4, 1.0, 8.0, seed=43)
+    b = gen.banded(20_000, 520, 4.0, 1.0, seed=44)
     st = spgemm_case(ctx, a, b)
     assert st["spgemm_direct_tiles"] == 0
 
@@ -183,7 +191,7 @@ def test_fused_tiled_multi_chunk(ctx, chunk_rows):
 def test_fused_direct_tiles_and_capacity_rerun(ctx, chunk_rows):
     # random columns: every sub-tile misses the staged path; the output exceeds
     # the speculative capacity, which is detected and re-run at the exact size
-    set_plan(ctx, (0, 0, 0), chunk_rows)
+    set_plan(ctx, (0, 0, 0, 1), chunk_rows)
     a = gen.random_matrix(2000, 8000, seed=45)
     b = gen.random_matrix(2000, 30000, seed=46)
     st = spgemm_case(ctx, a, b)
@@ -197,10 +205,50 @@ def test_algos_agree_on_cfg2_shape_sample(ctx):
     a = gen.banded(1 << 20, 512, 4.0, 32.0, seed=51)
     b = gen.banded(1 << 20, 512, 4.0, 32.0, seed=52)
     want = orc.spgemm(omat(a), omat(b), algo="hbv")
-    for algo in (0, 1):
-        set_plan(ctx, (algo, 0, 0))
+    for plan in FUSED + [(1, 0, 0)]:
+        set_plan(ctx, plan)
         got = ctx.spgemm(ctx.upload(a), ctx.upload(b)).download()
-        assert_same(got, want.rowmap, want.entries, want.nnz, f"algo {algo}")
+        assert_same(got, want.rowmap, want.entries, want.nnz, f"plan {plan}")
+
+
+@pytest.mark.parametrize("chunk_rows", [0, 2048])
+def test_fused_light_rows_wider_than_a_window_and_stage_overflow(ctx, chunk_rows):
+    # thread-per-row mode on rows spanning several 128-column windows, with
+    # more output than the chunk stage holds
+    set_plan(ctx, (0, 0, 0, 2), chunk_rows)
+    a = gen.banded(30_000, 300, 2.0, 1.0, seed=71)
+    b = gen.banded(30_000, 400, 6.0, 3.0, seed=72)
+    st = spgemm_case(ctx, a, b)
+    assert st["spgemm_light"] == 1
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("window", [(0, 1), (0, 5), (2, 9)])
+def test_index_of_noncanonical_and_cyclic_input(ctx, schedule, window):
+    # a random matrix (cycles) whose rows carry adjacent ranges: both
+    # schedules must reproduce the reference's canonical index
+    set_plan(ctx, (0, 0, 0, 0))
+    ctx.set_option("dindex_schedule", schedule)
+    a = gen.random_matrix(300, 900, seed=81)
+    ent = a.entries.copy()
+    rowmap = a.rowmap.copy()
+    # split the first multi-column range of every row into two adjacent ranges
+    out_e, out_r = [], [0]
+    for i in range(a.numRows()):
+        e = ent[int(rowmap[i]):int(rowmap[i + 1])].tolist()
+        split = False
+        for k in range(0, len(e), 2):
+            if not split and e[k + 1] > e[k]:
+                out_e += [e[k], e[k], e[k] + 1, e[k + 1]]
+                split = True
+            else:
+                out_e += [e[k], e[k + 1]]
+        out_r.append(len(out_e))
+    nc = CRSMatrix(a.numCols(), np.array(out_e, np.uint32), np.array(out_r, np.uint64))
+    want = orc.dindex(omat(nc), *window)
+    got = ctx.distance_index(ctx.upload(nc), *window).download()
+    assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
+    ctx.set_option("dindex_schedule", 0)
 
 
 def test_query_batch_matches_oracle(ctx):
