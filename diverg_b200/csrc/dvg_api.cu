@@ -214,11 +214,12 @@ static DeviceControl read_total(dvg_context* ctx, const uint64_t* rowmap_last, u
   return c;
 }
 
-static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b) {
+static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
+                                      const dvg_matrix* d = nullptr) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   // speculative output capacity; an overflow is detected and re-run exactly
   const uint64_t a_ent = a_identity ? 2ull * n : a->nentries;
-  uint64_t cap = std::max<uint64_t>({2 * a_ent, 2 * b->nentries, 4ull * n, 64});
+  uint64_t cap = std::max<uint64_t>({2 * a_ent, 2 * b->nentries, d ? 2 * d->nentries : 0, 4ull * n, 64});
   dvg_matrix* c = new_matrix(ctx, n, b->ncols, cap);
   try {
     DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
@@ -226,7 +227,7 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
     for (int attempt = 0; attempt < 2; ++attempt) {
       reset_control(ctx);
       cudaEvent_t t0 = span_begin(ctx);
-      launch_spgemm_fused(ctx, a, a_identity, b, c->rowmap, c->entries, cap);
+      launch_spgemm_fused(ctx, a, a_identity, b, d, c->rowmap, c->entries, cap);
       span_end(ctx, t0, kSymbolic);
       ctl = read_control(ctx);
       if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "range_spgemm: tile look-back wait expired");
@@ -244,14 +245,33 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
     ctx->stats.spgemm_calls++;
     ctx->stats.spgemm_direct_tiles += ctl.tiles_direct;
     ctx->stats.spgemm_slow_rows += ctl.slow_rows;
-    uint64_t bytes = (a_identity ? 0 : matrix_bytes(a)) + matrix_bytes(b) + matrix_bytes(c);
+    uint64_t bytes = (a_identity ? 0 : matrix_bytes(a)) + matrix_bytes(b) + matrix_bytes(c) + (d ? matrix_bytes(d) : 0);
     ctx->stats.alg_bytes += bytes;
     ctx->stats.spgemm_alg_bytes += bytes;
+    if (d) ctx->stats.spgemm_fused_adds++;
   } catch (...) {
     free_matrix(ctx, c);
     throw;
   }
   return c;
+}
+
+// C = D + A B as one canonical union.  The row kernel merges D's ranges into
+// each row's run list; the other kernels take the product and an SpAdd.  Only
+// the sum-of-powers schedule calls it, on canonical operands, where both give
+// the same canonical matrix.
+static dvg_matrix* range_spgemm_add(dvg_context* ctx, const dvg_matrix* d, const dvg_matrix* a, const dvg_matrix* b) {
+  require(a->ncols == b->nrows && d->nrows == a->nrows && d->ncols == b->ncols, "range_spgemm_add: shapes");
+  if (ctx->opt_algo == 0 && ctx->opt_spgemm_mode != 1) return range_spgemm_fused(ctx, a, false, b, d);
+  dvg_matrix* t = range_spgemm(ctx, a, false, b);
+  try {
+    dvg_matrix* c = range_spadd(ctx, d, t, false);
+    free_matrix(ctx, t);
+    return c;
+  } catch (...) {
+    free_matrix(ctx, t);
+    throw;
+  }
 }
 
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b) {
@@ -456,9 +476,7 @@ static dvg_matrix* distance_index_powersum(dvg_context* ctx, const dvg_matrix* a
           } else {
             // (A+I)^(e + 2^m) = (A+I)^e + A^e Q_m
             const dvg_matrix* Aexp = Ae ? Ae : P[__builtin_ctz(e)];
-            dvg_matrix* t = own(range_spgemm(ctx, Aexp, false, Q));
-            dvg_matrix* nr = own(range_spadd(ctx, R, t, false));
-            release(t);
+            dvg_matrix* nr = own(range_spgemm_add(ctx, R, Aexp, Q));
             if (R != Q) release(R);
             R = nr;
             // A^(e + 2^m) = A^e P_m, needed only for a later bit
@@ -472,9 +490,7 @@ static dvg_matrix* distance_index_powersum(dvg_context* ctx, const dvg_matrix* a
         }
         if (m < top_k) {
           // Q_(m+1) = Q_m + P_m Q_m
-          dvg_matrix* t = own(range_spgemm(ctx, P[m], false, Q));
-          dvg_matrix* nq = own(range_spadd(ctx, Q, t, false));
-          release(t);
+          dvg_matrix* nq = own(range_spgemm_add(ctx, Q, P[m], Q));
           if (Q != R) release(Q);
           Q = nq;
         }

@@ -134,8 +134,9 @@ void launch_spgemm(dvg_context* ctx, const SpgemmPlan& plan, const dvg_matrix* a
 // Fused single-pass SpGEMM (dvg_spgemm_fused.cu): writes c_rowmap fully and
 // c_entries up to `cap` entries; the control block receives the total entry
 // count, the nnz and an overflow flag when total > cap.
+// C = A B, or C = D + A B when d is not null (row kernel only)
 void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
-                         uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap);
+                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap);
 
 // Host orchestration (dvg_api.cu).
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b);

@@ -51,9 +51,8 @@ constexpr int kBMax = 768;        // B ranges staged per sub-tile
 constexpr int kBitWords = 6144;   // union bitmaps (PRE, SUF, BU) or direct windows
 constexpr int kStageMax = 6144;   // output entries staged per chunk
 constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
-constexpr int kRowWords = 6;      // row mode: 64-bit window words per thread (384 columns)
 constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
-constexpr int kSlot = 16;         // row mode: output entries kept per thread
+constexpr int kSlot = 24;         // row mode: output entries (run list) kept per thread
 constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
 constexpr unsigned long long kFlag = 1ull << 63;
 constexpr uint32_t kSpinLimit = 1u << 22;
@@ -81,8 +80,10 @@ struct FusedArgs {
   uint32_t nrows;
   uint32_t chunk_rows;  // multiple of kSubRows, <= kChunkMax
   uint32_t nchunks;
-  uint32_t row_mode;    // 1: a thread per row (shared window); 0: tile-staged rows
-  uint32_t row_words;   // row mode: 64-bit window words used per thread (<= kRowWords)
+  uint32_t row_mode;    // 1: a thread per row (run list); 0: tile-staged rows
+  // optional addend (row mode only): C = D + A B, D with the rows and columns of C
+  const uint64_t* __restrict__ d_rowmap;
+  const uint32_t* __restrict__ d_entries;
 };
 
 // One staged B window: rows [bs, bf] and their ranges.
@@ -329,6 +330,17 @@ __device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row
     b1 = p.b_rowmap[uint64_t(f) + 1] >> 1;
   };
   uint32_t mn = 0xffffffffu, mx = 0;
+  uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row
+  if (p.d_rowmap) {
+    d0 = p.d_rowmap[row] >> 1;
+    d1 = p.d_rowmap[row + 1] >> 1;
+  }
+  for (uint64_t t = d0 + lg; t < d1; t += 32) {
+    uint2 r = load_range(p.d_entries, t);
+    if (r.y < r.x) continue;
+    mn = min(mn, r.x);
+    mx = max(mx, r.y);
+  }
   for (uint64_t ai = a0; ai < a1; ai += 2) {
     uint64_t b0, b1;
     slice(ai, b0, b1);
@@ -355,25 +367,26 @@ __device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row
       reach[w] = 0;
     }
     __syncwarp();
+    auto put = [&](uint2 r) {
+      uint64_t cs = max(uint64_t(r.x), cb);
+      uint64_t cf = min(uint64_t(r.y), ce);
+      if (cs > cf || r.y < r.x) return;
+      uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
+      uint32_t lo = ~0u << (cs & 31);
+      uint32_t hi = ~0u >> (31 - (cf & 31));
+      if (ws == we) {
+        atomicOr(bits + ws, lo & hi);
+      } else {
+        atomicOr(bits + ws, lo);
+        atomicOr(bits + we, hi);
+        if (we > ws + 1) atomicMax(reach + ws + 1, we);
+      }
+    };
+    for (uint64_t t = d0 + lg; t < d1; t += 32) put(load_range(p.d_entries, t));
     for (uint64_t ai = a0; ai < a1; ai += 2) {
       uint64_t b0, b1;
       slice(ai, b0, b1);
-      for (uint64_t t = b0 + lg; t < b1; t += 32) {
-        uint2 r = load_range(p.b_entries, t);
-        uint64_t cs = max(uint64_t(r.x), cb);
-        uint64_t cf = min(uint64_t(r.y), ce);
-        if (cs > cf || r.y < r.x) continue;
-        uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
-        uint32_t lo = ~0u << (cs & 31);
-        uint32_t hi = ~0u >> (31 - (cf & 31));
-        if (ws == we) {
-          atomicOr(bits + ws, lo & hi);
-        } else {
-          atomicOr(bits + ws, lo);
-          atomicOr(bits + we, hi);
-          if (we > ws + 1) atomicMax(reach + ws + 1, we);
-        }
-      }
+      for (uint64_t t = b0 + lg; t < b1; t += 32) put(load_range(p.b_entries, t));
     }
     __syncwarp();
     uint32_t run_reach = 0;
@@ -530,8 +543,19 @@ __device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const F
     if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
     return a_staged ? achunk[k] : load_range(p.a_entries, k);
   };
+  uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row
+  if (p.d_rowmap) {
+    d0 = p.d_rowmap[row] >> 1;
+    d1 = p.d_rowmap[row + 1] >> 1;
+  }
   // column band of the row
   uint32_t lo = 0xffffffffu, hi = 0;
+  for (uint64_t t = d0; t < d1; ++t) {
+    const uint2 b = load_range(p.d_entries, t);
+    if (b.y < b.x) continue;
+    lo = min(lo, b.x);
+    hi = max(hi, b.y);
+  }
   for (uint64_t k = a0; k < a1; ++k) {
     const uint2 ar = a_range(k);
     if (ar.y < ar.x) continue;
@@ -548,18 +572,19 @@ __device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const F
   uint64_t carry = 0;
   for (uint64_t wb = lo & ~63u; wb <= hi; wb += 128) {
     uint64_t w0 = 0, w1 = 0;
+    auto put = [&](uint2 b) {
+      const uint64_t x = max(uint64_t(b.x), wb), y = min(uint64_t(b.y), wb + 127);
+      if (b.y < b.x || x > y) return;
+      const uint32_t xs = uint32_t(x - wb), ys = uint32_t(y - wb);
+      if (xs < 64) w0 |= (~0ull << xs) & (ys < 64 ? (~0ull >> (63 - ys)) : ~0ull);
+      if (ys >= 64) w1 |= (~0ull << (xs < 64 ? 0 : xs - 64)) & (~0ull >> (127 - ys));
+    };
+    for (uint64_t t = d0; t < d1; ++t) put(load_range(p.d_entries, t));
     for (uint64_t k = a0; k < a1; ++k) {
       const uint2 ar = a_range(k);
       if (ar.y < ar.x) continue;
       const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-      for (uint64_t t = t0; t < t1; ++t) {
-        const uint2 b = load_range(p.b_entries, t);
-        const uint64_t x = max(uint64_t(b.x), wb), y = min(uint64_t(b.y), wb + 127);
-        if (b.y < b.x || x > y) continue;
-        const uint32_t xs = uint32_t(x - wb), ys = uint32_t(y - wb);
-        if (xs < 64) w0 |= (~0ull << xs) & (ys < 64 ? (~0ull >> (63 - ys)) : ~0ull);
-        if (ys >= 64) w1 |= (~0ull << (xs < 64 ? 0 : xs - 64)) & (~0ull >> (127 - ys));
-      }
+      for (uint64_t t = t0; t < t1; ++t) put(load_range(p.b_entries, t));
     }
     if (nnz_acc) *nnz_acc += __popcll(w0) + __popcll(w1);
 #pragma unroll
@@ -584,29 +609,27 @@ __device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const F
   return count;
 }
 
-// ---- row mode: one C row by one thread, bitvector window in shared memory ---
+// ---- row mode: one C row by one thread, sorted run list in shared memory ----
 //
-// The row kernel below keeps its shared footprint small (a window, a reach
-// entry per window word and an output slot per thread, plus the chunk's row
-// counts) so that most of the SM's L1 caches the B ranges the threads read:
-// the lanes of a warp take consecutive rows, whose B slices overlap, and
-// neighbouring warps cover neighbouring rows.
-//
-// A thread's window covers row_words x 64 columns anchored 64 columns below
-// the row's first B range.  A B range [x, y] costs O(1) whatever its length:
-// its two edge words are ORed and the full words between them are recorded
-// as a reach entry (the last full word + 1) at the first of them; a running
-// maximum over reach while gathering turns them into full words.  The runs
-// are gathered with 64-bit map01 / map10 boundary masks and ffs and appended
-// to the thread's output slot at position `pos`.  row_fast returns false,
-// leaving no trace in nnz, when a range falls outside the window or the runs
-// overflow the slot; the caller then takes the windowed register path.
+// For the products of an index build the rows of C are a handful of runs,
+// however wide: the union is accumulated as a sorted list of disjoint,
+// non-adjacent runs -- exactly the canonical output -- held in the thread's
+// output slot.  A B range that overlaps or touches the open run (kept in
+// registers) extends it; any other range first merges the open run into the
+// list (insert, or merge with the runs it overlaps or touches: start <=
+// hi + 1, as the reference's accumulators merge).  The cost is output
+// sensitive and independent of the row's column span.  The shared footprint
+// is small (the slots, the chunk's row counts and the warp path's window), so
+// most of the SM's L1 caches the B ranges the threads read: the lanes of a
+// warp take consecutive rows, whose B slices overlap, and neighbouring warps
+// cover neighbouring rows.  row_runs returns false, leaving no trace in nnz,
+// when the runs overflow the slot; the row then goes to the warp path.
 constexpr int kRowRowsPerThread = kChunkMax / kThreads;
+constexpr int kRowDirectWW = 192;  // warp path: 32-bit window words per warp (6,144 columns)
 
 struct RowSmem {
-  uint64_t win[kRowWords * kThreads];   // word w of thread t at [w * kThreads + t]
-  uint16_t reach[kRowWords * kThreads];
-  uint32_t slot[kSlot * kThreads];
+  uint32_t slot[kSlot * kThreads];      // entry k of thread t at [k * kThreads + t]
+  uint32_t direct[2 * kRowDirectWW * kWarps];  // warp path: bits + reach per warp
   uint32_t incl[kChunkMax];
   uint32_t slow[kSlowMax];              // rows left to the warp-cooperative path
   unsigned long long red[kWarps];
@@ -614,19 +637,12 @@ struct RowSmem {
   uint32_t chunk;
   uint32_t nslow;
 };
-// the warp-cooperative path reuses the row windows: 32-bit bits + reach per warp
-constexpr int kRowDirectWW = int(sizeof(uint64_t) * kRowWords * kThreads / sizeof(uint32_t)) / (2 * kWarps);
 
-// base_hint: ~0 anchors the window 64 columns below the row's first B range;
-// any other value is the window's first column (a multiple of 64).
 template <bool A_ID>
-__device__ bool row_fast(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
-                         unsigned long long& nnz, uint64_t base_hint) {
-  const int tid = threadIdx.x;
-  uint64_t* win = S.win + tid;
-  uint16_t* reach = S.reach + tid;
-  uint32_t* slot = S.slot + tid;
-  const uint32_t W = p.row_words;
+__device__ bool row_runs(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
+                         unsigned long long& nnz) {
+  uint32_t* L = S.slot + threadIdx.x + size_t(pos) * kThreads;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
+  const uint32_t max_runs = (uint32_t(kSlot) - pos) >> 1;
   uint64_t a0, a1;
   if (A_ID) {
     a0 = 0;
@@ -635,131 +651,79 @@ __device__ bool row_fast(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t 
     a0 = __ldg(p.a_rowmap + row) >> 1;
     a1 = __ldg(p.a_rowmap + row + 1) >> 1;
   }
-  for (uint32_t w = 0; w < W; ++w) {
-    win[w * kThreads] = 0;
-    reach[w * kThreads] = 0;
-  }
-  const uint64_t cols = 64ull * W;
-  uint64_t base = 0;
-  bool any = false;
-  uint32_t wtop = 0;
-  // the open run, kept in registers: ranges that overlap or touch it extend
-  // it; any other range first flushes it into the window
-  uint32_t run_lo = 0, run_hi = 0;
-  auto flush = [&](uint32_t x, uint32_t y) {
-    const uint32_t xs = uint32_t(x - base), ys = uint32_t(y - base);
-    const uint32_t ws = xs >> 6, we = ys >> 6;
-    const uint64_t lo = ~0ull << (xs & 63), hi = ~0ull >> (63 - (ys & 63));
-    if (ws == we) {
-      win[ws * kThreads] |= lo & hi;
-    } else {
-      win[ws * kThreads] |= lo;
-      win[we * kThreads] |= hi;
-      if (we > ws + 1) {
-        uint16_t& rr = reach[(ws + 1) * kThreads];
-        if (rr < we) rr = uint16_t(we);
+  uint32_t nr = 0;
+  // merges [x, y] into the list; false when it needs more runs than fit
+  auto merge = [&](uint32_t x, uint32_t y) -> bool {
+    uint32_t k = 0;
+    while (k < nr && uint64_t(L[(2 * k + 1) * kThreads]) + 1 < x) ++k;
+    if (k == nr || uint64_t(y) + 1 < L[2 * k * kThreads]) {
+      if (nr == max_runs) return false;
+      for (uint32_t m = nr; m > k; --m) {
+        L[2 * m * kThreads] = L[2 * (m - 1) * kThreads];
+        L[(2 * m + 1) * kThreads] = L[(2 * m - 1) * kThreads];
       }
+      L[2 * k * kThreads] = x;
+      L[(2 * k + 1) * kThreads] = y;
+      ++nr;
+      return true;
     }
-    wtop = max(wtop, we);
+    uint32_t lo = min(L[2 * k * kThreads], x), hi = max(L[(2 * k + 1) * kThreads], y);
+    uint32_t m = k + 1;
+    while (m < nr && uint64_t(hi) + 1 >= L[2 * m * kThreads]) {
+      hi = max(hi, L[(2 * m + 1) * kThreads]);
+      ++m;
+    }
+    L[2 * k * kThreads] = lo;
+    L[(2 * k + 1) * kThreads] = hi;
+    const uint32_t gone = m - k - 1;
+    if (gone) {
+      for (uint32_t q = m; q < nr; ++q) {
+        L[2 * (q - gone) * kThreads] = L[2 * q * kThreads];
+        L[(2 * (q - gone) + 1) * kThreads] = L[(2 * q + 1) * kThreads];
+      }
+      nr -= gone;
+    }
+    return true;
   };
-  for (uint64_t k = a0; k < a1; ++k) {
-    const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
-    if (ar.y < ar.x) continue;
-    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-    for (uint64_t t = t0; t < t1; ++t) {
-      const uint2 b = load_range(p.b_entries, t);
-      if (b.y < b.x) continue;
-      if (!any) {
-        any = true;
-        base = base_hint != ~0ull ? base_hint : (b.x >= 64 ? (uint64_t(b.x) & ~63ull) - 64 : 0);
-        run_lo = b.x;
-        run_hi = b.y;
-        continue;
-      }
-      if (uint64_t(b.x) <= uint64_t(run_hi) + 1 && uint64_t(b.y) + 1 >= run_lo) {
-        run_lo = min(run_lo, b.x);
-        run_hi = max(run_hi, b.y);
-        continue;
-      }
-      // merging may have carried the open run past the window: every flush
-      // checks the run it writes
-      if (run_lo < base || uint64_t(run_hi) >= base + cols) return false;
-      flush(run_lo, run_hi);
+  bool any = false;
+  uint32_t run_lo = 0, run_hi = 0;
+  // one input range: extend the open run, or merge the open run and open anew
+  auto take = [&](uint2 b) -> bool {
+    if (b.y < b.x) return true;
+    if (!any) {
+      any = true;
       run_lo = b.x;
       run_hi = b.y;
+      return true;
     }
-  }
-  if (any) {
-    if (run_lo < base || uint64_t(run_hi) >= base + cols) return false;
-    flush(run_lo, run_hi);
-  }
-  count = 0;
-  if (!any) return true;
-  uint64_t carry = 0, n = 0;
-  uint32_t run = 0, c = 0;
-  for (uint32_t w = 0; w <= wtop; ++w) {
-    uint64_t x = win[w * kThreads];
-    run = max(run, uint32_t(reach[w * kThreads]));
-    if (run > w) x = ~0ull;
-    n += __popcll(x);
-    const uint64_t sh = (x << 1) | carry;
-    uint64_t bnd = ((x ^ sh) & x) | (sh & ~x);
-    while (bnd) {
-      const int bit = __ffsll(bnd) - 1;
-      bnd &= bnd - 1;
-      if (pos + c >= uint32_t(kSlot)) return false;
-      slot[(pos + c) * kThreads] = uint32_t(base + 64ull * w + bit - (c & 1));
-      ++c;
+    if (uint64_t(b.x) <= uint64_t(run_hi) + 1 && uint64_t(b.y) + 1 >= run_lo) {
+      run_lo = min(run_lo, b.x);
+      run_hi = max(run_hi, b.y);
+      return true;
     }
-    carry = x >> 63;
+    if (!merge(run_lo, run_hi)) return false;
+    run_lo = b.x;
+    run_hi = b.y;
+    return true;
+  };
+  if (p.d_rowmap) {
+    const uint64_t d0 = __ldg(p.d_rowmap + row) >> 1, d1 = __ldg(p.d_rowmap + row + 1) >> 1;
+    for (uint64_t t = d0; t < d1; ++t)
+      if (!take(load_range(p.d_entries, t))) return false;
   }
-  if (carry) {  // the run reaching the end of word wtop closes there
-    if (pos + c >= uint32_t(kSlot)) return false;
-    slot[(pos + c) * kThreads] = uint32_t(base + 64ull * wtop + 63);
-    ++c;
-  }
-  count = c;
-  nnz += n;
-  return true;
-}
-
-// Exact column band [lo, hi] of a C row (lo > hi when the row is empty).
-template <bool A_ID>
-__device__ void row_band(const FusedArgs& p, uint64_t row, uint32_t& lo, uint32_t& hi) {
-  uint64_t a0, a1;
-  if (A_ID) {
-    a0 = 0;
-    a1 = 1;
-  } else {
-    a0 = __ldg(p.a_rowmap + row) >> 1;
-    a1 = __ldg(p.a_rowmap + row + 1) >> 1;
-  }
-  lo = 0xffffffffu;
-  hi = 0;
   for (uint64_t k = a0; k < a1; ++k) {
     const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
     if (ar.y < ar.x) continue;
     const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-    for (uint64_t t = t0; t < t1; ++t) {
-      const uint2 b = load_range(p.b_entries, t);
-      if (b.y < b.x) continue;
-      lo = min(lo, b.x);
-      hi = max(hi, b.y);
-    }
+    for (uint64_t t = t0; t < t1; ++t)
+      if (!take(load_range(p.b_entries, t))) return false;
   }
-}
-
-// Fast path with one retry anchored at the row's exact band.
-template <bool A_ID>
-__device__ bool row_fast_retry(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
-                               unsigned long long& nnz) {
-  if (row_fast<A_ID>(S, p, row, pos, count, nnz, ~0ull)) return true;
-  uint32_t lo, hi;
-  row_band<A_ID>(p, row, lo, hi);
-  if (lo > hi) return false;
-  const uint64_t base = uint64_t(lo) & ~63ull;
-  if (uint64_t(hi) >= base + 64ull * p.row_words) return false;
-  return row_fast<A_ID>(S, p, row, pos, count, nnz, base);
+  if (any && !merge(run_lo, run_hi)) return false;
+  uint64_t n = 0;
+  for (uint32_t k = 0; k < nr; ++k) n += uint64_t(L[(2 * k + 1) * kThreads]) - L[2 * k * kThreads] + 1;
+  count = 2 * nr;
+  nnz += n;
+  return true;
 }
 
 // The row kernel: chunks from the ticket; thread (warp, lane) owns chunk rows
@@ -770,7 +734,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RowSmem& S = *reinterpret_cast<RowSmem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  uint32_t* dbits = reinterpret_cast<uint32_t*>(S.win) + size_t(warp) * 2 * kRowDirectWW;
+  uint32_t* dbits = S.direct + size_t(warp) * 2 * kRowDirectWW;
   uint32_t* dreach = dbits + kRowDirectWW;
   while (true) {
     if (tid == 0) {
@@ -791,7 +755,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
       if (r < crows) {
         uint32_t cnt = 0;
-        if (row_fast_retry<A_ID>(S, p, uint64_t(c0row) + r, pos, cnt, nnz_acc)) {
+        if (row_runs<A_ID>(S, p, uint64_t(c0row) + r, pos, cnt, nnz_acc)) {
           fast_mask |= 1u << u;
           pos += cnt;
         } else {
@@ -1257,11 +1221,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_fused(FusedArgs p) {
 }  // namespace
 
 void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
-                         uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
+                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   if (n == 0) return;
-  // row mode unless the tiled mode is requested
+  // row mode unless the tiled mode is requested; an addend needs row mode
   const bool row_mode = ctx->opt_spgemm_mode != 1;
+  if (d && !row_mode) throw Error(DVG_ERR_INVALID_ARG, "fused spgemm: an addend needs the row kernel");
   auto kern = row_mode ? (a_identity ? k_spgemm_rowmode<true> : k_spgemm_rowmode<false>)
                        : (a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>);
   const int smem = int(row_mode ? sizeof(RowSmem) : sizeof(Smem));
@@ -1303,7 +1268,8 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
   p.chunk_rows = chunk_rows;
   p.nchunks = nchunks;
   p.row_mode = row_mode ? 1u : 0u;
-  p.row_words = kRowWords;
+  p.d_rowmap = d ? d->rowmap : nullptr;
+  p.d_entries = d ? d->entries : nullptr;
   if (row_mode) ctx->stats.spgemm_light++;
   const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
   kern<<<grid, kThreads, smem, ctx->stream>>>(p);
@@ -1464,8 +1430,7 @@ extern "C" dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncol
     p.chunk_rows = chunk_rows;
     p.nchunks = nchunks;
     p.row_mode = 0;
-    p.row_words = kRowWords;
-    const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
+      const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
     kern<<<grid, kThreads, smem, stream>>>(p);
     DVG_CUDA(cudaGetLastError());
     DVG_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, stream));

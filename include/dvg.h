@@ -64,9 +64,10 @@ typedef struct dvg_stats {
   uint64_t spgemm_direct_tiles; /* SpGEMM row tiles that missed the staged path */
   uint64_t spgemm_reruns;       /* SpGEMMs re-run after an output capacity overflow */
   uint64_t spgemm_light;        /* SpGEMMs run in the thread-per-row mode */
-  uint64_t spgemm_slow_rows;    /* thread-per-row rows that took the windowed fallback */
+  uint64_t spgemm_slow_rows;    /* thread-per-row rows that missed the run list (warp path) */
   uint64_t host_alloc_ns;       /* host time spent in device allocation calls */
   uint64_t host_sync_ns;        /* host time spent waiting on stream synchronisation */
+  uint64_t spgemm_fused_adds;   /* products computed as D + A B in one pass */
 } dvg_stats;
 
 /* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /

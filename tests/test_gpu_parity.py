@@ -251,6 +251,23 @@ def test_index_of_noncanonical_and_cyclic_input(ctx, schedule, window):
     ctx.set_option("dindex_schedule", 0)
 
 
+@pytest.mark.parametrize("chunk_rows", [0, 2048])
+@pytest.mark.parametrize("window", [(0, 4), (2, 5)])
+def test_index_fused_sums_on_fragmented_rows(ctx, window, chunk_rows):
+    # random columns: the rows of every product hold more runs than a thread's
+    # list, so the sums D + A B of the sum-of-powers schedule take the warp
+    # path and, past its per-chunk list, the per-thread windowed path
+    set_plan(ctx, (0, 0, 0, 0), chunk_rows)
+    ctx.set_option("dindex_schedule", 0)
+    a = gen.random_matrix(6000, 30000, seed=83)
+    want = orc.dindex(omat(a), *window)
+    ctx.reset_stats()
+    got = ctx.distance_index(ctx.upload(a), *window).download()
+    st = ctx.stats()
+    assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
+    assert st["spgemm_fused_adds"] > 0 and st["spgemm_slow_rows"] > 2048
+
+
 def test_query_batch_matches_oracle(ctx):
     a, _ = gen.graph_adjacency(gen.small_graph_spec(50_000, seed=4))
     idx = orc.dindex(omat(a), 100, 300, algo="hbv")
