@@ -56,7 +56,7 @@ void cuda_check(cudaError_t e, const char* what) {
   throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-static uint64_t now_ns() {
+uint64_t now_ns() {
   return uint64_t(std::chrono::duration_cast<std::chrono::nanoseconds>(
                       std::chrono::steady_clock::now().time_since_epoch()).count());
 }
@@ -115,10 +115,6 @@ void dfree(dvg_context* ctx, void* p) {
   ctx->live_blocks.erase(it);
 }
 
-static size_t entries_alloc_bytes(uint64_t nentries) {
-  // padded to 16 bytes so vector loads of the last range stay inside
-  return size_t((nentries * 4 + 15) / 16 * 16 + 16);
-}
 
 dvg_matrix* new_matrix(dvg_context* ctx, uint32_t nrows, uint32_t ncols, uint64_t nentries) {
   auto* m = new dvg_matrix();
@@ -171,7 +167,7 @@ void span_end(dvg_context* ctx, cudaEvent_t begin, TimedKind kind) {
 }
 
 // After a stream synchronisation every recorded span has completed.
-static void resolve_spans(dvg_context* ctx) {
+void resolve_spans(dvg_context* ctx) {
   for (auto& t : ctx->timed) {
     float ms = 0.f;
     DVG_CUDA(cudaEventElapsedTime(&ms, t.begin, t.end));
@@ -242,6 +238,7 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
     c->nentries = ctl.total;
     c->nnz = ctl.nnz;
     c->canonical = true;
+    ctx->max_product_entries = std::max(ctx->max_product_entries, c->nentries);
     ctx->stats.spgemm_calls++;
     ctx->stats.spgemm_direct_tiles += ctl.tiles_direct;
     ctx->stats.spgemm_slow_rows += ctl.slow_rows;
@@ -538,6 +535,32 @@ dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigne
   // canonical only for canonical inputs, while the reference's squarings
   // canonicalise any input
   if (ctx->opt_dindex_schedule == 1 || (dlo == 0 && !a->canonical)) return distance_index_reference(ctx, a, dlo, dup);
+  if (ctx->opt_planned && ctx->opt_algo == 0 && ctx->opt_spgemm_mode != 1 && a->nrows > 0) {
+    PlannedBuild pb;
+    bool planned = true;
+    try {
+      pb = prepare_build(ctx, plan_index(dlo, dup), a);
+    } catch (const Error& e) {
+      if (e.status != DVG_ERR_OOM) throw;
+      planned = false;  // the estimates do not fit: exact sizes on the read-back path
+    }
+    if (!planned) return distance_index_powersum(ctx, a, dlo, dup);
+    try {
+      launch_build(ctx, pb, ctx->opt_timing);
+    } catch (...) {
+      release_build(ctx, pb);
+      throw;
+    }
+    if (dvg_matrix* t = finish_build(ctx, pb)) return t;
+    // a step outgrew its estimate: build on the read-back path and size the
+    // next planned builds from its largest product
+    ctx->stats.spgemm_reruns++;
+    ctx->max_product_entries = 0;
+    dvg_matrix* t = distance_index_powersum(ctx, a, dlo, dup);
+    const double grow = double(ctx->max_product_entries) / double(std::max<uint64_t>(a->nentries, 1));
+    ctx->plan_growth = std::max(ctx->plan_growth, 1.25 * grow + 0.25);
+    return t;
+  }
   return distance_index_powersum(ctx, a, dlo, dup);
 }
 
@@ -615,6 +638,7 @@ dvg_status dvg_shutdown(dvg_context* ctx) {
     ctx->event_pool.clear();
     DVG_CUDA(cudaFree(ctx->d_ctl));
     DVG_CUDA(cudaFreeHost(ctx->h_ctl));
+    if (ctx->h_stage) DVG_CUDA(cudaFreeHost(ctx->h_stage));
     if (ctx->own_stream) DVG_CUDA(cudaStreamDestroy(ctx->own_stream));
   });
   delete ctx;
@@ -657,6 +681,15 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "spgemm_mode")) {
       require(value >= 0 && value <= 2, "spgemm_mode must be 0 (automatic), 1 (tiled) or 2 (light)");
       ctx->opt_spgemm_mode = value;
+    } else if (!std::strcmp(key, "planned_build")) {
+      require(value == 0 || value == 1, "planned_build must be 0 or 1");
+      ctx->opt_planned = value;
+    } else if (!std::strcmp(key, "plan_growth")) {
+      require(value >= 0 && value <= 100000, "plan_growth is a percentage in [0, 100000]");
+      ctx->plan_growth = double(value) / 100.0;
+    } else if (!std::strcmp(key, "row_slot")) {
+      require(value >= 0 && value <= 2, "row_slot must be 0 (16 entries), 1 (24) or 2 (32)");
+      ctx->opt_row_slot = value;
     } else if (!std::strcmp(key, "chunk_rows")) {
       require(value >= 0 && value <= 2048 && value % 32 == 0, "chunk_rows must be 0 or a multiple of 32 up to 2048");
       ctx->opt_chunk_rows = value;

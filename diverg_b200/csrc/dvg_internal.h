@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <unordered_map>
 #include <stdexcept>
@@ -39,6 +40,12 @@ struct DeviceControl {
   unsigned long long slow_rows;     // row-mode rows that missed the shared window
 };
 
+// A row-kernel shape chosen by the autotuner.
+struct TuneChoice {
+  int slot_variant;    // run-list entries per thread: 0 -> 16, 1 -> 24, 2 -> 32
+  int64_t chunk_rows;  // 0: automatic
+};
+
 struct dvg_context {
   int device = 0;
   int num_sms = 0;
@@ -62,6 +69,15 @@ struct dvg_context {
   int64_t opt_chunk_rows = 0;         // fused SpGEMM look-back chunk rows (0: automatic)
   int64_t opt_spgemm_mode = 0;        // fused SpGEMM: 0 automatic, 1 tiled, 2 light
   int64_t opt_dindex_schedule = 0;    // 0: sum of powers, 1: the reference's squaring
+  int64_t opt_row_slot = 1;           // row kernel run-list width variant (0: 16, 1: 24, 2: 32 entries)
+  uint32_t row_resident[3] = {0, 0, 0};  // resident CTAs of the row kernel per variant
+  int64_t opt_planned = 1;            // 1: index builds run planned (no host round trips)
+  double plan_growth = 3.0;           // planned builds: entry capacity per step / input entries
+  uint64_t max_product_entries = 0;   // largest product output since the last reset (read-back path)
+  int64_t opt_autotune = 1;           // batches: tune the row kernel per (window, size class)
+  std::map<std::tuple<unsigned, unsigned, int>, TuneChoice> tuned;
+  void* h_stage = nullptr;            // pinned host staging for read-backs
+  size_t h_stage_cap = 0;
   bool opt_timing = false;
   // event pairs bracketing timed kernels, resolved at the next stream sync
   struct TimedSpan {
@@ -138,6 +154,38 @@ void launch_spgemm(dvg_context* ctx, const SpgemmPlan& plan, const dvg_matrix* a
 void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
                          const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap);
 
+// Thread-per-row single-pass product (dvg_spgemm_rows.cu) on raw arrays:
+// C = A B, C = D + A B, or C = I + A B (d_identity); A may be the identity.
+// The caller provides zeroed chunk descriptors (desc_bytes of the shape), a
+// zeroed ticket and the control block the kernel reports into; `abort`, when
+// not null, is checked before any work and set when C is unusable.
+struct RowLaunch {
+  const uint64_t* a_rowmap = nullptr;
+  const uint32_t* a_entries = nullptr;
+  bool a_identity = false;
+  const uint64_t* b_rowmap = nullptr;
+  const uint32_t* b_entries = nullptr;
+  const uint64_t* d_rowmap = nullptr;
+  const uint32_t* d_entries = nullptr;
+  bool d_identity = false;
+  uint64_t* c_rowmap = nullptr;
+  uint32_t* c_entries = nullptr;
+  uint64_t cap = 0;
+  uint32_t nrows = 0;
+  void* desc = nullptr;
+  unsigned* ticket = nullptr;
+  DeviceControl* ctl = nullptr;
+  unsigned long long* abort = nullptr;
+  int slot_variant = 1;  // run-list entries per thread: 0 -> 16, 1 -> 24, 2 -> 32
+};
+struct RowLaunchShape {
+  uint32_t resident, chunk_rows, nchunks, grid;
+  size_t desc_bytes;
+};
+RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_rows_opt, int slot_variant);
+void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& shape);
+int row_slot_entries(int variant);
+
 // Host orchestration (dvg_api.cu).
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b);
 dvg_matrix* range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity);
@@ -147,5 +195,72 @@ dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigne
 inline uint64_t matrix_bytes(const dvg_matrix* m) {
   return 8ull * (uint64_t(m->nrows) + 1) + 4ull * m->nentries;
 }
+
+// Bytes allocated for `nentries` entries: padded to 16 bytes so vector loads
+// of the last range stay inside.
+inline size_t entries_alloc_bytes(uint64_t nentries) { return size_t((nentries * 4 + 15) / 16 * 16 + 16); }
+
+uint64_t now_ns();
+// Folds the completed event spans into the statistics (after a stream sync).
+void resolve_spans(dvg_context* ctx);
+// Pinned host staging of at least `bytes` (grown on demand).
+void* host_stage(dvg_context* ctx, size_t bytes);
+
+// ---- planned builds (dvg_engine.cu) -----------------------------------------
+// The index schedule as a fixed sequence of thread-per-row products whose
+// buffers are all allocated before the first launch, so the whole build runs
+// without a host round trip (and can be captured in a CUDA graph).  Output
+// capacities are estimated; a step whose output overflows sets a device word
+// that makes every later step return at once, and the host then re-runs the
+// build on the synchronised path.
+struct PlanStep {
+  int c, a, b, d;      // slots: output, left factor, right factor, addend (-1: none)
+  bool a_id, d_id;     // left factor / addend is the identity
+};
+struct IndexPlan {
+  std::vector<PlanStep> steps;
+  int nslots = 1;      // slot 0 is the adjacency matrix
+  int out = -1;        // slot of the index
+};
+IndexPlan plan_index(unsigned dlo, unsigned dup);
+
+struct PlannedBuild {
+  IndexPlan plan;
+  const dvg_matrix* input = nullptr;
+  uint32_t n = 0;
+  std::vector<uint64_t*> rowmap;    // per slot, as the launches use them (slot 0: the input's)
+  std::vector<uint32_t*> entries;
+  std::vector<char> live;           // the slot still owns its buffers (not yet handed back)
+  std::vector<uint64_t> cap;        // entry capacity per slot
+  std::vector<int> owner_step;      // producing step per slot (-1: input)
+  RowLaunchShape shape{};
+  int slot_variant = 1;
+  void* scratch = nullptr;          // chunk descriptors | tickets | controls | abort word
+  size_t scratch_bytes = 0;
+  size_t desc_stride = 0;
+  unsigned* tickets = nullptr;
+  DeviceControl* ctls = nullptr;
+  unsigned long long* abort = nullptr;
+};
+// Allocates every buffer of the plan for input `a` (no device work beyond
+// stream-ordered allocation).
+PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_matrix* a);
+// The same with the row kernel's run-list width variant and chunk rows given.
+PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_matrix* a, int slot_variant,
+                           int64_t chunk_rows);
+// Issues the build: one memset and one kernel per step, no host round trip.
+void launch_build(dvg_context* ctx, PlannedBuild& pb, bool timed);
+// Reads the step controls back (one synchronisation), releases the
+// intermediates and returns the index, or nullptr after an overflow (all
+// buffers released).
+dvg_matrix* finish_build(dvg_context* ctx, PlannedBuild& pb);
+void release_build(dvg_context* ctx, PlannedBuild& pb);
+
+// ---- batches (dvg_batch.cu) ----------------------------------------------------
+// Fastest row-kernel shape for planned builds of `a`'s size class and window,
+// timed once per context and kept.
+TuneChoice autotune_build(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup);
+void batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* const* graphs, const unsigned* dmin,
+                          const unsigned* dmax, dvg_matrix** out);
 
 }  // namespace dvg

@@ -1,0 +1,391 @@
+// dvg_spgemm_common.cuh -- pieces shared by the two single-pass range SpGEMM
+// kernels (tile-staged: dvg_spgemm_fused.cu; thread per row:
+// dvg_spgemm_rows.cu): launch constants, the chunk descriptors of the
+// decoupled look-back, the kernel arguments, the warp-cooperative row path for
+// rows too wide for the fast paths, the look-back itself and the per-thread
+// windowed fallback.  Included by both translation units (internal linkage).
+#pragma once
+
+#include "dvg_device.cuh"
+#include "dvg_internal.h"
+
+namespace dvg {
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+constexpr int kSubRows = 64;      // rows per staged sub-tile
+constexpr int kChunkMax = 2048;   // rows per look-back chunk (upper bound)
+constexpr int kSubMax = kChunkMax / kSubRows;
+constexpr int kAChunk = 3072;     // A ranges staged per chunk
+constexpr int kSpanMax = 384;     // B rows staged per sub-tile
+constexpr int kBMax = 768;        // B ranges staged per sub-tile
+constexpr int kBitWords = 6144;   // union bitmaps (PRE, SUF, BU) or direct windows
+constexpr int kStageMax = 6144;   // output entries staged per chunk
+constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
+constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
+constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
+constexpr unsigned long long kFlag = 1ull << 63;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+struct ChunkDesc {
+  unsigned long long agg;       // kFlag | entries of the chunk
+  unsigned long long agg_nnz;
+  unsigned long long incl;      // kFlag | entries of chunks 0..t
+  unsigned long long incl_nnz;
+};
+
+struct FusedArgs {
+  const uint64_t* __restrict__ a_rowmap;
+  const uint32_t* __restrict__ a_entries;
+  const uint64_t* __restrict__ b_rowmap;
+  const uint32_t* __restrict__ b_entries;
+  uint64_t* __restrict__ c_rowmap;
+  uint32_t* __restrict__ c_entries;
+  uint64_t cap;
+  ChunkDesc* desc;
+  unsigned* ticket;
+  DeviceControl* ctl;
+  uint32_t nrows;
+  uint32_t chunk_rows;  // multiple of kSubRows, <= kChunkMax
+  uint32_t nchunks;
+  uint32_t row_mode;    // 1: a thread per row (run list); 0: tile-staged rows
+  // optional addend (row mode only): C = D + A B, D with the rows and columns of C
+  const uint64_t* __restrict__ d_rowmap;
+  const uint32_t* __restrict__ d_entries;
+  uint32_t d_identity;  // the addend is the identity (d_rowmap unused)
+  // planned builds: a word every step checks before it starts and sets when
+  // its output is unusable (overflow, timeout, internal error); null otherwise
+  unsigned long long* abort;
+};
+
+// Records an error bit in the control block field and, in a planned build,
+// stops the steps that follow.
+__device__ __forceinline__ void raise_flag(const FusedArgs& p, unsigned long long* field, unsigned long long bits) {
+  atomicOr(field, bits);
+  if (p.abort) atomicOr(p.abort, 1ull);
+}
+
+// ---- small helpers -----------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Gathers the runs of one 32-bit accumulator word per lane of a group of g lanes
+// (map01 / map10 boundary masks, ffs); see the callers.
+template <class Emit>
+__device__ __forceinline__ uint32_t gather_chunk(uint32_t x, bool valid, uint64_t c0, int g, int lg, unsigned gm,
+                                                 uint32_t& carry, uint64_t count, uint32_t last_lane, Emit&& emit) {
+  uint32_t prev = __shfl_up_sync(gm, x, 1, g);
+  uint32_t c = lg == 0 ? carry : (prev >> 31);
+  uint32_t sh = (x << 1) | c;
+  uint32_t bnd = valid ? (((x ^ sh) & x) | (sh & ~x)) : 0u;
+  uint32_t cnt = __popc(bnd);
+  uint32_t incl = cnt;
+  for (int o = 1; o < g; o <<= 1) {
+    uint32_t u = __shfl_up_sync(gm, incl, o, g);
+    if (lg >= o) incl += u;
+  }
+  uint64_t k = count + incl - cnt;
+  while (bnd) {
+    int bit = __ffs(bnd) - 1;
+    bnd &= bnd - 1;
+    emit(k, uint32_t(c0 + bit - (k & 1)));
+    ++k;
+  }
+  uint32_t total = __shfl_sync(gm, incl, g - 1, g);
+  carry = __shfl_sync(gm, x, int(last_lane), g) >> 31;
+  return total;
+}
+
+// ---- direct path: one C row by a warp, bitvector window in shared memory ----
+
+template <class Emit>
+__device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row, uint32_t* bits, uint32_t* reach,
+                               unsigned long long* nnz_acc, Emit&& emit, uint32_t ww = kDirectWW) {
+  const int lg = lane_id();
+  uint64_t a0, a1;
+  if (a_identity) {
+    a0 = 0;
+    a1 = 2;
+  } else {
+    a0 = p.a_rowmap[row];
+    a1 = p.a_rowmap[row + 1];
+  }
+  auto slice = [&](uint64_t ai, uint64_t& b0, uint64_t& b1) {
+    uint32_t s, f;
+    if (a_identity) {
+      s = f = uint32_t(row);
+    } else {
+      uint2 r = load_range(p.a_entries, ai >> 1);
+      s = r.x;
+      f = r.y;
+    }
+    if (f < s) {
+      b0 = b1 = 0;
+      return;
+    }
+    b0 = p.b_rowmap[s] >> 1;
+    b1 = p.b_rowmap[uint64_t(f) + 1] >> 1;
+  };
+  uint32_t mn = 0xffffffffu, mx = 0;
+  uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row
+  if (p.d_rowmap) {
+    d0 = p.d_rowmap[row] >> 1;
+    d1 = p.d_rowmap[row + 1] >> 1;
+  }
+  for (uint64_t t = d0 + lg; t < d1; t += 32) {
+    uint2 r = load_range(p.d_entries, t);
+    if (r.y < r.x) continue;
+    mn = min(mn, r.x);
+    mx = max(mx, r.y);
+  }
+  if (p.d_identity && lg == 0) {
+    mn = min(mn, uint32_t(row));
+    mx = max(mx, uint32_t(row));
+  }
+  for (uint64_t ai = a0; ai < a1; ai += 2) {
+    uint64_t b0, b1;
+    slice(ai, b0, b1);
+    for (uint64_t t = b0 + lg; t < b1; t += 32) {
+      uint2 r = load_range(p.b_entries, t);
+      if (r.y < r.x) continue;
+      mn = min(mn, r.x);
+      mx = max(mx, r.y);
+    }
+  }
+  mn = group_min<32>(kFullMask, mn);
+  mx = group_max<32>(kFullMask, mx);
+  uint64_t count = 0;
+  if (mn > mx) return 0;
+  const uint64_t base = mn & ~31u;
+  const uint64_t nw_total = ((uint64_t(mx) - base) >> 5) + 2;
+  uint32_t carry = 0;
+  for (uint64_t w0 = 0; w0 < nw_total; w0 += ww) {
+    const uint32_t nwc = uint32_t(min(uint64_t(ww), nw_total - w0));
+    const uint64_t cb = base + 32 * w0;
+    const uint64_t ce = cb + 32ull * nwc - 1;
+    for (uint32_t w = lg; w < nwc; w += 32) {
+      bits[w] = 0;
+      reach[w] = 0;
+    }
+    __syncwarp();
+    auto put = [&](uint2 r) {
+      uint64_t cs = max(uint64_t(r.x), cb);
+      uint64_t cf = min(uint64_t(r.y), ce);
+      if (cs > cf || r.y < r.x) return;
+      uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
+      uint32_t lo = ~0u << (cs & 31);
+      uint32_t hi = ~0u >> (31 - (cf & 31));
+      if (ws == we) {
+        atomicOr(bits + ws, lo & hi);
+      } else {
+        atomicOr(bits + ws, lo);
+        atomicOr(bits + we, hi);
+        if (we > ws + 1) atomicMax(reach + ws + 1, we);
+      }
+    };
+    for (uint64_t t = d0 + lg; t < d1; t += 32) put(load_range(p.d_entries, t));
+    if (p.d_identity && lg == 0) put(make_uint2(uint32_t(row), uint32_t(row)));
+    for (uint64_t ai = a0; ai < a1; ai += 2) {
+      uint64_t b0, b1;
+      slice(ai, b0, b1);
+      for (uint64_t t = b0 + lg; t < b1; t += 32) put(load_range(p.b_entries, t));
+    }
+    __syncwarp();
+    uint32_t run_reach = 0;
+    for (uint32_t wb = 0; wb < nwc; wb += 32) {
+      const uint32_t w = wb + lg;
+      const bool valid = w < nwc;
+      uint32_t x = 0, rr = 0;
+      if (valid) {
+        x = bits[w];
+        rr = reach[w];
+      }
+      rr = group_incl_max<32>(kFullMask, rr, lg);
+      rr = max(rr, run_reach);
+      if (valid && rr > w) x = ~0u;
+      run_reach = __shfl_sync(kFullMask, rr, 31);
+      if (nnz_acc) *nnz_acc += __popc(x);
+      const uint32_t last = min(31u, nwc - 1 - wb);
+      count += gather_chunk(x, valid, cb + 32ull * w, 32, lg, kFullMask, carry, count, last, emit);
+    }
+    __syncwarp();
+  }
+  return count;
+}
+
+// ---- warp-parallel decoupled look-back over the chunk order -----------------
+// Called by one full warp; every lane returns the chunk's exclusive prefix.
+__device__ void lookback_warp(const FusedArgs& p, uint32_t t, unsigned long long cnt, unsigned long long nnz,
+                              unsigned long long& prefix, unsigned long long& prefix_nnz) {
+  const int lane = lane_id();
+  ChunkDesc* d = p.desc;
+  unsigned long long pre = 0, pre_nnz = 0;
+  if (t != 0) {
+    if (lane == 0) {
+      d[t].agg_nnz = nnz;
+      st_release(&d[t].agg, kFlag | cnt);
+    }
+    int64_t j = int64_t(t) - 1;
+    uint32_t spins = 0;
+    while (true) {
+      const int64_t idx = j - lane;
+      int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: not yet
+      unsigned long long v = 0, vn = 0;
+      if (idx >= 0) {
+        unsigned long long vi = ld_acquire(&d[idx].incl);
+        if (vi & kFlag) {
+          v = vi & ~kFlag;
+          vn = *reinterpret_cast<volatile unsigned long long*>(&d[idx].incl_nnz);
+        } else {
+          unsigned long long va = ld_acquire(&d[idx].agg);
+          if (va & kFlag) {
+            st = 1;
+            v = va & ~kFlag;
+            vn = *reinterpret_cast<volatile unsigned long long*>(&d[idx].agg_nnz);
+          } else {
+            st = 0;
+          }
+        }
+      }
+      const unsigned incl_mask = __ballot_sync(kFullMask, st == 2);
+      const unsigned wait_mask = __ballot_sync(kFullMask, st == 0);
+      const int first = incl_mask ? __ffs(incl_mask) - 1 : 32;
+      const unsigned before = first == 32 ? kFullMask : ((1u << first) - 1u);
+      if (wait_mask & before) {
+        if (++spins > kSpinLimit) {
+          if (lane == 0) raise_flag(p, &p.ctl->timeout, 1ull);
+          break;
+        }
+        __nanosleep(32);
+        continue;
+      }
+      unsigned long long sv = lane <= first ? v : 0ull, sn = lane <= first ? vn : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sv += __shfl_xor_sync(kFullMask, sv, o);
+        sn += __shfl_xor_sync(kFullMask, sn, o);
+      }
+      pre += sv;
+      pre_nnz += sn;
+      if (first < 32) break;
+      j -= 32;
+    }
+  }
+  if (lane == 0) {
+    d[t].incl_nnz = pre_nnz + nnz;
+    st_release(&d[t].incl, kFlag | (pre + cnt));
+  }
+  prefix = pre;
+  prefix_nnz = pre_nnz;
+}
+
+// ---- light path: one C row by one thread --------------------------------------
+//
+// For products whose rows union only a handful of B ranges (powers of A, the
+// final A^d * (A+I)^k product) a thread per row beats any cooperative scheme:
+// the row's ranges -- read from the staged chunk of A and from B through L1 --
+// are ORed into a 128-column register bitmap anchored at the row's first
+// column; the runs come out with the same boundary masks as the tiled gather,
+// on 64-bit words.  Rows wider than the window take further 128-column
+// windows, each re-reading the row's ranges.
+template <bool A_ID, class Emit>
+__device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const FusedArgs& p, uint32_t c0row,
+                              uint32_t r, bool a_staged, unsigned long long* nnz_acc, Emit&& emit) {
+  const uint64_t row = uint64_t(c0row) + r;
+  uint64_t a0, a1;
+  if (A_ID) {
+    a0 = 0;
+    a1 = 1;
+  } else if (a_staged) {
+    a0 = crow[r] >> 1;
+    a1 = crow[r + 1] >> 1;
+  } else {
+    a0 = p.a_rowmap[row] >> 1;
+    a1 = p.a_rowmap[row + 1] >> 1;
+  }
+  auto a_range = [&](uint64_t k) -> uint2 {
+    if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
+    return a_staged ? achunk[k] : load_range(p.a_entries, k);
+  };
+  uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row
+  if (p.d_rowmap) {
+    d0 = p.d_rowmap[row] >> 1;
+    d1 = p.d_rowmap[row + 1] >> 1;
+  }
+  // column band of the row
+  uint32_t lo = 0xffffffffu, hi = 0;
+  for (uint64_t t = d0; t < d1; ++t) {
+    const uint2 b = load_range(p.d_entries, t);
+    if (b.y < b.x) continue;
+    lo = min(lo, b.x);
+    hi = max(hi, b.y);
+  }
+  if (p.d_identity) {
+    lo = min(lo, uint32_t(row));
+    hi = max(hi, uint32_t(row));
+  }
+  for (uint64_t k = a0; k < a1; ++k) {
+    const uint2 ar = a_range(k);
+    if (ar.y < ar.x) continue;
+    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    for (uint64_t t = t0; t < t1; ++t) {
+      const uint2 b = load_range(p.b_entries, t);
+      if (b.y < b.x) continue;
+      lo = min(lo, b.x);
+      hi = max(hi, b.y);
+    }
+  }
+  if (lo > hi) return 0;
+  uint32_t count = 0;
+  uint64_t carry = 0;
+  for (uint64_t wb = lo & ~63u; wb <= hi; wb += 128) {
+    uint64_t w0 = 0, w1 = 0;
+    auto put = [&](uint2 b) {
+      const uint64_t x = max(uint64_t(b.x), wb), y = min(uint64_t(b.y), wb + 127);
+      if (b.y < b.x || x > y) return;
+      const uint32_t xs = uint32_t(x - wb), ys = uint32_t(y - wb);
+      if (xs < 64) w0 |= (~0ull << xs) & (ys < 64 ? (~0ull >> (63 - ys)) : ~0ull);
+      if (ys >= 64) w1 |= (~0ull << (xs < 64 ? 0 : xs - 64)) & (~0ull >> (127 - ys));
+    };
+    for (uint64_t t = d0; t < d1; ++t) put(load_range(p.d_entries, t));
+    if (p.d_identity) put(make_uint2(uint32_t(row), uint32_t(row)));
+    for (uint64_t k = a0; k < a1; ++k) {
+      const uint2 ar = a_range(k);
+      if (ar.y < ar.x) continue;
+      const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+      for (uint64_t t = t0; t < t1; ++t) put(load_range(p.b_entries, t));
+    }
+    if (nnz_acc) *nnz_acc += __popcll(w0) + __popcll(w1);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint64_t x = h ? w1 : w0;
+      const uint64_t sh = (x << 1) | carry;
+      uint64_t bnd = ((x ^ sh) & x) | (sh & ~x);
+      const uint64_t c0 = wb + 64 * h;
+      while (bnd) {
+        const int bit = __ffsll(bnd) - 1;
+        bnd &= bnd - 1;
+        emit(count, uint32_t(c0 + bit - (count & 1)));
+        ++count;
+      }
+      carry = x >> 63;
+    }
+  }
+  if (carry) {  // a run reaching the last window's end closes at column hi
+    emit(count, hi);
+    ++count;
+  }
+  return count;
+}
+
+}  // namespace
+}  // namespace dvg

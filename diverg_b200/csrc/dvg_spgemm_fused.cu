@@ -34,57 +34,12 @@
 #include <algorithm>
 #include <mutex>
 
-#include "dvg_device.cuh"
-#include "dvg_internal.h"
+#include "dvg_spgemm_common.cuh"
 
 namespace dvg {
 namespace {
 
-constexpr int kThreads = 512;
-constexpr int kWarps = kThreads / 32;
-constexpr int kSubRows = 64;      // rows per staged sub-tile
-constexpr int kChunkMax = 2048;   // rows per look-back chunk (upper bound)
-constexpr int kSubMax = kChunkMax / kSubRows;
-constexpr int kAChunk = 3072;     // A ranges staged per chunk
-constexpr int kSpanMax = 384;     // B rows staged per sub-tile
-constexpr int kBMax = 768;        // B ranges staged per sub-tile
-constexpr int kBitWords = 6144;   // union bitmaps (PRE, SUF, BU) or direct windows
-constexpr int kStageMax = 6144;   // output entries staged per chunk
-constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
-constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
-constexpr int kSlot = 24;         // row mode: output entries (run list) kept per thread
-constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
-constexpr unsigned long long kFlag = 1ull << 63;
-constexpr uint32_t kSpinLimit = 1u << 22;
-
 enum TileMode : uint32_t { kTiled = 0, kDirect = 1, kEmpty = 2 };
-
-struct ChunkDesc {
-  unsigned long long agg;       // kFlag | entries of the chunk
-  unsigned long long agg_nnz;
-  unsigned long long incl;      // kFlag | entries of chunks 0..t
-  unsigned long long incl_nnz;
-};
-
-struct FusedArgs {
-  const uint64_t* __restrict__ a_rowmap;
-  const uint32_t* __restrict__ a_entries;
-  const uint64_t* __restrict__ b_rowmap;
-  const uint32_t* __restrict__ b_entries;
-  uint64_t* __restrict__ c_rowmap;
-  uint32_t* __restrict__ c_entries;
-  uint64_t cap;
-  ChunkDesc* desc;
-  unsigned* ticket;
-  DeviceControl* ctl;
-  uint32_t nrows;
-  uint32_t chunk_rows;  // multiple of kSubRows, <= kChunkMax
-  uint32_t nchunks;
-  uint32_t row_mode;    // 1: a thread per row (run list); 0: tile-staged rows
-  // optional addend (row mode only): C = D + A B, D with the rows and columns of C
-  const uint64_t* __restrict__ d_rowmap;
-  const uint32_t* __restrict__ d_entries;
-};
 
 // One staged B window: rows [bs, bf] and their ranges.
 struct BBuf {
@@ -201,16 +156,6 @@ __device__ unsigned long long block_sum(Smem& S, unsigned long long v) {
   return s;
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
 // ---- tiled path ----------------------------------------------------------------
 
 struct TileGeom {
@@ -257,33 +202,6 @@ __device__ __forceinline__ uint32_t tiled_acc(const Smem& S, const TileGeom& T, 
 // Emits through `emit(row_local_index, value)`; returns the chunk's boundary
 // count (group-uniform) and updates `carry` (msb of the chunk's last word).
 template <class Emit>
-__device__ __forceinline__ uint32_t gather_chunk(uint32_t x, bool valid, uint64_t c0, int g, int lg, unsigned gm,
-                                                 uint32_t& carry, uint64_t count, uint32_t last_lane, Emit&& emit) {
-  uint32_t prev = __shfl_up_sync(gm, x, 1, g);
-  uint32_t c = lg == 0 ? carry : (prev >> 31);
-  uint32_t sh = (x << 1) | c;
-  uint32_t bnd = valid ? (((x ^ sh) & x) | (sh & ~x)) : 0u;
-  uint32_t cnt = __popc(bnd);
-  uint32_t incl = cnt;
-  for (int o = 1; o < g; o <<= 1) {
-    uint32_t u = __shfl_up_sync(gm, incl, o, g);
-    if (lg >= o) incl += u;
-  }
-  uint64_t k = count + incl - cnt;
-  while (bnd) {
-    int bit = __ffs(bnd) - 1;
-    bnd &= bnd - 1;
-    emit(k, uint32_t(c0 + bit - (k & 1)));
-    ++k;
-  }
-  uint32_t total = __shfl_sync(gm, incl, g - 1, g);
-  carry = __shfl_sync(gm, x, int(last_lane), g) >> 31;
-  return total;
-}
-
-// C row r of a tiled sub-tile, window chunk by window chunk.  Returns the
-// entry count; adds the row's nnz into *nnz_acc (per lane) when given.
-template <class Emit>
 __device__ uint32_t tiled_row(const Smem& S, const TileGeom& T, uint32_t r, int g, int lg, unsigned gm,
                               unsigned long long* nnz_acc, Emit&& emit) {
   uint32_t carry = 0;
@@ -297,184 +215,6 @@ __device__ uint32_t tiled_row(const Smem& S, const TileGeom& T, uint32_t r, int 
     count += gather_chunk(x, valid, T.base + 32ull * w, g, lg, gm, carry, count, last, emit);
   }
   return uint32_t(count);
-}
-
-// ---- direct path: one C row by a warp, bitvector window in shared memory ----
-
-template <class Emit>
-__device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row, uint32_t* bits, uint32_t* reach,
-                               unsigned long long* nnz_acc, Emit&& emit, uint32_t ww = kDirectWW) {
-  const int lg = lane_id();
-  uint64_t a0, a1;
-  if (a_identity) {
-    a0 = 0;
-    a1 = 2;
-  } else {
-    a0 = p.a_rowmap[row];
-    a1 = p.a_rowmap[row + 1];
-  }
-  auto slice = [&](uint64_t ai, uint64_t& b0, uint64_t& b1) {
-    uint32_t s, f;
-    if (a_identity) {
-      s = f = uint32_t(row);
-    } else {
-      uint2 r = load_range(p.a_entries, ai >> 1);
-      s = r.x;
-      f = r.y;
-    }
-    if (f < s) {
-      b0 = b1 = 0;
-      return;
-    }
-    b0 = p.b_rowmap[s] >> 1;
-    b1 = p.b_rowmap[uint64_t(f) + 1] >> 1;
-  };
-  uint32_t mn = 0xffffffffu, mx = 0;
-  uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row
-  if (p.d_rowmap) {
-    d0 = p.d_rowmap[row] >> 1;
-    d1 = p.d_rowmap[row + 1] >> 1;
-  }
-  for (uint64_t t = d0 + lg; t < d1; t += 32) {
-    uint2 r = load_range(p.d_entries, t);
-    if (r.y < r.x) continue;
-    mn = min(mn, r.x);
-    mx = max(mx, r.y);
-  }
-  for (uint64_t ai = a0; ai < a1; ai += 2) {
-    uint64_t b0, b1;
-    slice(ai, b0, b1);
-    for (uint64_t t = b0 + lg; t < b1; t += 32) {
-      uint2 r = load_range(p.b_entries, t);
-      if (r.y < r.x) continue;
-      mn = min(mn, r.x);
-      mx = max(mx, r.y);
-    }
-  }
-  mn = group_min<32>(kFullMask, mn);
-  mx = group_max<32>(kFullMask, mx);
-  uint64_t count = 0;
-  if (mn > mx) return 0;
-  const uint64_t base = mn & ~31u;
-  const uint64_t nw_total = ((uint64_t(mx) - base) >> 5) + 2;
-  uint32_t carry = 0;
-  for (uint64_t w0 = 0; w0 < nw_total; w0 += ww) {
-    const uint32_t nwc = uint32_t(min(uint64_t(ww), nw_total - w0));
-    const uint64_t cb = base + 32 * w0;
-    const uint64_t ce = cb + 32ull * nwc - 1;
-    for (uint32_t w = lg; w < nwc; w += 32) {
-      bits[w] = 0;
-      reach[w] = 0;
-    }
-    __syncwarp();
-    auto put = [&](uint2 r) {
-      uint64_t cs = max(uint64_t(r.x), cb);
-      uint64_t cf = min(uint64_t(r.y), ce);
-      if (cs > cf || r.y < r.x) return;
-      uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
-      uint32_t lo = ~0u << (cs & 31);
-      uint32_t hi = ~0u >> (31 - (cf & 31));
-      if (ws == we) {
-        atomicOr(bits + ws, lo & hi);
-      } else {
-        atomicOr(bits + ws, lo);
-        atomicOr(bits + we, hi);
-        if (we > ws + 1) atomicMax(reach + ws + 1, we);
-      }
-    };
-    for (uint64_t t = d0 + lg; t < d1; t += 32) put(load_range(p.d_entries, t));
-    for (uint64_t ai = a0; ai < a1; ai += 2) {
-      uint64_t b0, b1;
-      slice(ai, b0, b1);
-      for (uint64_t t = b0 + lg; t < b1; t += 32) put(load_range(p.b_entries, t));
-    }
-    __syncwarp();
-    uint32_t run_reach = 0;
-    for (uint32_t wb = 0; wb < nwc; wb += 32) {
-      const uint32_t w = wb + lg;
-      const bool valid = w < nwc;
-      uint32_t x = 0, rr = 0;
-      if (valid) {
-        x = bits[w];
-        rr = reach[w];
-      }
-      rr = group_incl_max<32>(kFullMask, rr, lg);
-      rr = max(rr, run_reach);
-      if (valid && rr > w) x = ~0u;
-      run_reach = __shfl_sync(kFullMask, rr, 31);
-      if (nnz_acc) *nnz_acc += __popc(x);
-      const uint32_t last = min(31u, nwc - 1 - wb);
-      count += gather_chunk(x, valid, cb + 32ull * w, 32, lg, kFullMask, carry, count, last, emit);
-    }
-    __syncwarp();
-  }
-  return count;
-}
-
-// ---- warp-parallel decoupled look-back over the chunk order -----------------
-// Called by one full warp; every lane returns the chunk's exclusive prefix.
-__device__ void lookback_warp(const FusedArgs& p, uint32_t t, unsigned long long cnt, unsigned long long nnz,
-                              unsigned long long& prefix, unsigned long long& prefix_nnz) {
-  const int lane = lane_id();
-  ChunkDesc* d = p.desc;
-  unsigned long long pre = 0, pre_nnz = 0;
-  if (t != 0) {
-    if (lane == 0) {
-      d[t].agg_nnz = nnz;
-      st_release(&d[t].agg, kFlag | cnt);
-    }
-    int64_t j = int64_t(t) - 1;
-    uint32_t spins = 0;
-    while (true) {
-      const int64_t idx = j - lane;
-      int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: not yet
-      unsigned long long v = 0, vn = 0;
-      if (idx >= 0) {
-        unsigned long long vi = ld_acquire(&d[idx].incl);
-        if (vi & kFlag) {
-          v = vi & ~kFlag;
-          vn = *reinterpret_cast<volatile unsigned long long*>(&d[idx].incl_nnz);
-        } else {
-          unsigned long long va = ld_acquire(&d[idx].agg);
-          if (va & kFlag) {
-            st = 1;
-            v = va & ~kFlag;
-            vn = *reinterpret_cast<volatile unsigned long long*>(&d[idx].agg_nnz);
-          } else {
-            st = 0;
-          }
-        }
-      }
-      const unsigned incl_mask = __ballot_sync(kFullMask, st == 2);
-      const unsigned wait_mask = __ballot_sync(kFullMask, st == 0);
-      const int first = incl_mask ? __ffs(incl_mask) - 1 : 32;
-      const unsigned before = first == 32 ? kFullMask : ((1u << first) - 1u);
-      if (wait_mask & before) {
-        if (++spins > kSpinLimit) {
-          if (lane == 0) atomicOr(&p.ctl->timeout, 1ull);
-          break;
-        }
-        __nanosleep(32);
-        continue;
-      }
-      unsigned long long sv = lane <= first ? v : 0ull, sn = lane <= first ? vn : 0ull;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        sv += __shfl_xor_sync(kFullMask, sv, o);
-        sn += __shfl_xor_sync(kFullMask, sn, o);
-      }
-      pre += sv;
-      pre_nnz += sn;
-      if (first < 32) break;
-      j -= 32;
-    }
-  }
-  if (lane == 0) {
-    d[t].incl_nnz = pre_nnz + nnz;
-    st_release(&d[t].incl, kFlag | (pre + cnt));
-  }
-  prefix = pre;
-  prefix_nnz = pre_nnz;
 }
 
 // Warp 0: stage offsets for the sub-tile's rows [r0, r0 + rows) (rows <= 64,
@@ -512,378 +252,6 @@ __device__ void stage_rows(Smem& S, uint32_t r0, uint32_t rows) {
     S.stage_used = uint32_t(used + fit_end);
     if (nfit < rows) S.stage_open = 0;
     S.staged_rows += nfit;
-  }
-}
-
-// ---- light path: one C row by one thread --------------------------------------
-//
-// For products whose rows union only a handful of B ranges (powers of A, the
-// final A^d * (A+I)^k product) a thread per row beats any cooperative scheme:
-// the row's ranges -- read from the staged chunk of A and from B through L1 --
-// are ORed into a 128-column register bitmap anchored at the row's first
-// column; the runs come out with the same boundary masks as the tiled gather,
-// on 64-bit words.  Rows wider than the window take further 128-column
-// windows, each re-reading the row's ranges.
-template <bool A_ID, class Emit>
-__device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const FusedArgs& p, uint32_t c0row,
-                              uint32_t r, bool a_staged, unsigned long long* nnz_acc, Emit&& emit) {
-  const uint64_t row = uint64_t(c0row) + r;
-  uint64_t a0, a1;
-  if (A_ID) {
-    a0 = 0;
-    a1 = 1;
-  } else if (a_staged) {
-    a0 = crow[r] >> 1;
-    a1 = crow[r + 1] >> 1;
-  } else {
-    a0 = p.a_rowmap[row] >> 1;
-    a1 = p.a_rowmap[row + 1] >> 1;
-  }
-  auto a_range = [&](uint64_t k) -> uint2 {
-    if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
-    return a_staged ? achunk[k] : load_range(p.a_entries, k);
-  };
-  uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row
-  if (p.d_rowmap) {
-    d0 = p.d_rowmap[row] >> 1;
-    d1 = p.d_rowmap[row + 1] >> 1;
-  }
-  // column band of the row
-  uint32_t lo = 0xffffffffu, hi = 0;
-  for (uint64_t t = d0; t < d1; ++t) {
-    const uint2 b = load_range(p.d_entries, t);
-    if (b.y < b.x) continue;
-    lo = min(lo, b.x);
-    hi = max(hi, b.y);
-  }
-  for (uint64_t k = a0; k < a1; ++k) {
-    const uint2 ar = a_range(k);
-    if (ar.y < ar.x) continue;
-    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-    for (uint64_t t = t0; t < t1; ++t) {
-      const uint2 b = load_range(p.b_entries, t);
-      if (b.y < b.x) continue;
-      lo = min(lo, b.x);
-      hi = max(hi, b.y);
-    }
-  }
-  if (lo > hi) return 0;
-  uint32_t count = 0;
-  uint64_t carry = 0;
-  for (uint64_t wb = lo & ~63u; wb <= hi; wb += 128) {
-    uint64_t w0 = 0, w1 = 0;
-    auto put = [&](uint2 b) {
-      const uint64_t x = max(uint64_t(b.x), wb), y = min(uint64_t(b.y), wb + 127);
-      if (b.y < b.x || x > y) return;
-      const uint32_t xs = uint32_t(x - wb), ys = uint32_t(y - wb);
-      if (xs < 64) w0 |= (~0ull << xs) & (ys < 64 ? (~0ull >> (63 - ys)) : ~0ull);
-      if (ys >= 64) w1 |= (~0ull << (xs < 64 ? 0 : xs - 64)) & (~0ull >> (127 - ys));
-    };
-    for (uint64_t t = d0; t < d1; ++t) put(load_range(p.d_entries, t));
-    for (uint64_t k = a0; k < a1; ++k) {
-      const uint2 ar = a_range(k);
-      if (ar.y < ar.x) continue;
-      const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-      for (uint64_t t = t0; t < t1; ++t) put(load_range(p.b_entries, t));
-    }
-    if (nnz_acc) *nnz_acc += __popcll(w0) + __popcll(w1);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const uint64_t x = h ? w1 : w0;
-      const uint64_t sh = (x << 1) | carry;
-      uint64_t bnd = ((x ^ sh) & x) | (sh & ~x);
-      const uint64_t c0 = wb + 64 * h;
-      while (bnd) {
-        const int bit = __ffsll(bnd) - 1;
-        bnd &= bnd - 1;
-        emit(count, uint32_t(c0 + bit - (count & 1)));
-        ++count;
-      }
-      carry = x >> 63;
-    }
-  }
-  if (carry) {  // a run reaching the last window's end closes at column hi
-    emit(count, hi);
-    ++count;
-  }
-  return count;
-}
-
-// ---- row mode: one C row by one thread, sorted run list in shared memory ----
-//
-// For the products of an index build the rows of C are a handful of runs,
-// however wide: the union is accumulated as a sorted list of disjoint,
-// non-adjacent runs -- exactly the canonical output -- held in the thread's
-// output slot.  A B range that overlaps or touches the open run (kept in
-// registers) extends it; any other range first merges the open run into the
-// list (insert, or merge with the runs it overlaps or touches: start <=
-// hi + 1, as the reference's accumulators merge).  The cost is output
-// sensitive and independent of the row's column span.  The shared footprint
-// is small (the slots, the chunk's row counts and the warp path's window), so
-// most of the SM's L1 caches the B ranges the threads read: the lanes of a
-// warp take consecutive rows, whose B slices overlap, and neighbouring warps
-// cover neighbouring rows.  row_runs returns false, leaving no trace in nnz,
-// when the runs overflow the slot; the row then goes to the warp path.
-constexpr int kRowRowsPerThread = kChunkMax / kThreads;
-constexpr int kRowDirectWW = 192;  // warp path: 32-bit window words per warp (6,144 columns)
-
-struct RowSmem {
-  uint32_t slot[kSlot * kThreads];      // entry k of thread t at [k * kThreads + t]
-  uint32_t direct[2 * kRowDirectWW * kWarps];  // warp path: bits + reach per warp
-  uint32_t incl[kChunkMax];
-  uint32_t slow[kSlowMax];              // rows left to the warp-cooperative path
-  unsigned long long red[kWarps];
-  unsigned long long prefix;
-  uint32_t chunk;
-  uint32_t nslow;
-};
-
-template <bool A_ID>
-__device__ bool row_runs(RowSmem& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
-                         unsigned long long& nnz) {
-  uint32_t* L = S.slot + threadIdx.x + size_t(pos) * kThreads;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
-  const uint32_t max_runs = (uint32_t(kSlot) - pos) >> 1;
-  uint64_t a0, a1;
-  if (A_ID) {
-    a0 = 0;
-    a1 = 1;
-  } else {
-    a0 = __ldg(p.a_rowmap + row) >> 1;
-    a1 = __ldg(p.a_rowmap + row + 1) >> 1;
-  }
-  uint32_t nr = 0;
-  // merges [x, y] into the list; false when it needs more runs than fit
-  auto merge = [&](uint32_t x, uint32_t y) -> bool {
-    uint32_t k = 0;
-    while (k < nr && uint64_t(L[(2 * k + 1) * kThreads]) + 1 < x) ++k;
-    if (k == nr || uint64_t(y) + 1 < L[2 * k * kThreads]) {
-      if (nr == max_runs) return false;
-      for (uint32_t m = nr; m > k; --m) {
-        L[2 * m * kThreads] = L[2 * (m - 1) * kThreads];
-        L[(2 * m + 1) * kThreads] = L[(2 * m - 1) * kThreads];
-      }
-      L[2 * k * kThreads] = x;
-      L[(2 * k + 1) * kThreads] = y;
-      ++nr;
-      return true;
-    }
-    uint32_t lo = min(L[2 * k * kThreads], x), hi = max(L[(2 * k + 1) * kThreads], y);
-    uint32_t m = k + 1;
-    while (m < nr && uint64_t(hi) + 1 >= L[2 * m * kThreads]) {
-      hi = max(hi, L[(2 * m + 1) * kThreads]);
-      ++m;
-    }
-    L[2 * k * kThreads] = lo;
-    L[(2 * k + 1) * kThreads] = hi;
-    const uint32_t gone = m - k - 1;
-    if (gone) {
-      for (uint32_t q = m; q < nr; ++q) {
-        L[2 * (q - gone) * kThreads] = L[2 * q * kThreads];
-        L[(2 * (q - gone) + 1) * kThreads] = L[(2 * q + 1) * kThreads];
-      }
-      nr -= gone;
-    }
-    return true;
-  };
-  bool any = false;
-  uint32_t run_lo = 0, run_hi = 0;
-  // one input range: extend the open run, or merge the open run and open anew
-  auto take = [&](uint2 b) -> bool {
-    if (b.y < b.x) return true;
-    if (!any) {
-      any = true;
-      run_lo = b.x;
-      run_hi = b.y;
-      return true;
-    }
-    if (uint64_t(b.x) <= uint64_t(run_hi) + 1 && uint64_t(b.y) + 1 >= run_lo) {
-      run_lo = min(run_lo, b.x);
-      run_hi = max(run_hi, b.y);
-      return true;
-    }
-    if (!merge(run_lo, run_hi)) return false;
-    run_lo = b.x;
-    run_hi = b.y;
-    return true;
-  };
-  if (p.d_rowmap) {
-    const uint64_t d0 = __ldg(p.d_rowmap + row) >> 1, d1 = __ldg(p.d_rowmap + row + 1) >> 1;
-    for (uint64_t t = d0; t < d1; ++t)
-      if (!take(load_range(p.d_entries, t))) return false;
-  }
-  for (uint64_t k = a0; k < a1; ++k) {
-    const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
-    if (ar.y < ar.x) continue;
-    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-    for (uint64_t t = t0; t < t1; ++t)
-      if (!take(load_range(p.b_entries, t))) return false;
-  }
-  if (any && !merge(run_lo, run_hi)) return false;
-  uint64_t n = 0;
-  for (uint32_t k = 0; k < nr; ++k) n += uint64_t(L[(2 * k + 1) * kThreads]) - L[2 * k * kThreads] + 1;
-  count = 2 * nr;
-  nnz += n;
-  return true;
-}
-
-// The row kernel: chunks from the ticket; thread (warp, lane) owns chunk rows
-// (warp * kRowRowsPerThread + u) * 32 + lane; counts, chunk prefix, look-back,
-// then every thread writes its rows from its slot (or recomputes them).
-template <bool A_ID>
-__global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  RowSmem& S = *reinterpret_cast<RowSmem*>(smem_raw);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  uint32_t* dbits = S.direct + size_t(warp) * 2 * kRowDirectWW;
-  uint32_t* dreach = dbits + kRowDirectWW;
-  while (true) {
-    if (tid == 0) {
-      S.chunk = atomicAdd(p.ticket, 1u);
-      S.nslow = 0;
-    }
-    __syncthreads();
-    const uint32_t t = S.chunk;
-    if (t >= p.nchunks) break;
-    const uint32_t c0row = t * p.chunk_rows;
-    const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
-    unsigned long long nnz_acc = 0;
-    uint32_t fast_mask = 0, pos = 0;
-    // rows that miss the window wait for the warp-cooperative pass below, so
-    // one wide row never holds a whole chunk behind a single thread
-#pragma unroll
-    for (int u = 0; u < kRowRowsPerThread; ++u) {
-      const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
-      if (r < crows) {
-        uint32_t cnt = 0;
-        if (row_runs<A_ID>(S, p, uint64_t(c0row) + r, pos, cnt, nnz_acc)) {
-          fast_mask |= 1u << u;
-          pos += cnt;
-        } else {
-          const uint32_t i = atomicAdd(&S.nslow, 1u);
-          if (i < uint32_t(kSlowMax)) {
-            S.slow[i] = r;
-          } else {
-            cnt = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
-          }
-          atomicAdd(&p.ctl->slow_rows, 1ull);
-        }
-        S.incl[r] = cnt;
-      }
-    }
-    __syncthreads();
-    const uint32_t nslow = min(S.nslow, uint32_t(kSlowMax));
-    for (uint32_t i = warp; i < nslow; i += kWarps) {
-      const uint32_t r = S.slow[i];
-      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
-                                    [](uint64_t, uint32_t) {}, kRowDirectWW);
-      if (lane == 0) S.incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
-    }
-    __syncthreads();
-    // chunk prefix over the row counts (kRowRowsPerThread consecutive rows per thread)
-    {
-      uint32_t loc[kRowRowsPerThread];
-      uint64_t s = 0;
-#pragma unroll
-      for (int k = 0; k < kRowRowsPerThread; ++k) {
-        const uint32_t r = tid * kRowRowsPerThread + k;
-        s += r < crows ? S.incl[r] : 0u;
-        loc[k] = uint32_t(s);
-      }
-      uint64_t inc = s;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint64_t u = __shfl_up_sync(kFullMask, inc, o);
-        if (lane >= o) inc += u;
-      }
-      if (lane == 31) S.red[warp] = inc;
-      __syncthreads();
-      uint64_t wpre = 0;
-      for (int i = 0; i < warp; ++i) wpre += S.red[i];
-      const uint64_t excl = wpre + inc - s;
-      if (excl + s > 0xffffffffull) atomicOr(&p.ctl->status, 16ull);
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < kRowRowsPerThread; ++k) {
-        const uint32_t r = tid * kRowRowsPerThread + k;
-        if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
-      }
-    }
-    // chunk nnz
-    unsigned long long v = nnz_acc;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
-    if (lane == 0) S.red[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-      unsigned long long chunk_nnz = 0;
-      for (int i = 0; i < kWarps; ++i) chunk_nnz += S.red[i];
-      const unsigned long long chunk_cnt = S.incl[crows - 1];
-      unsigned long long pre, pre_nnz;
-      lookback_warp(p, t, chunk_cnt, chunk_nnz, pre, pre_nnz);
-      if (lane == 0) {
-        S.prefix = pre;
-        if (t == p.nchunks - 1) {
-          p.ctl->total = pre + chunk_cnt;
-          p.ctl->nnz = pre_nnz + chunk_nnz;
-          if (pre + chunk_cnt > p.cap) p.ctl->overflow = pre + chunk_cnt;
-        }
-      }
-    }
-    __syncthreads();
-    const unsigned long long prefix = S.prefix;
-    for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
-    if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
-    pos = 0;
-#pragma unroll
-    for (int u = 0; u < kRowRowsPerThread; ++u) {
-      const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
-      if (r >= crows) continue;
-      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
-      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
-      const bool fast = (fast_mask >> u) & 1u;
-      if (n && dst + n > p.cap) {
-        atomicOr(&p.ctl->overflow, 1ull);
-      } else if (fast) {
-        for (uint32_t k = 0; k < n; ++k) p.c_entries[dst + k] = S.slot[(pos + k) * kThreads + tid];
-      }
-      if (fast) pos += n;
-    }
-    // rows that missed the window: the listed ones by warps, any overflow of
-    // the list by its own thread
-    for (uint32_t i = warp; i < nslow; i += kWarps) {
-      const uint32_t r = S.slow[i];
-      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
-      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
-      if (n == 0 || dst + n > p.cap) continue;
-      uint32_t* out = p.c_entries + dst;
-      bool bad = false;
-      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
-                                    [&](uint64_t k, uint32_t v) {
-                                      if (k < n) out[k] = v;
-                                      else bad = true;
-                                    },
-                                    kRowDirectWW);
-      if (bad || c != n) atomicOr(&p.ctl->status, 8ull);
-    }
-    if (S.nslow > uint32_t(kSlowMax)) {
-#pragma unroll
-      for (int u = 0; u < kRowRowsPerThread; ++u) {
-        const uint32_t r = (warp * kRowRowsPerThread + u) * 32 + lane;
-        if (r >= crows || ((fast_mask >> u) & 1u)) continue;
-        bool listed = false;
-        for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
-        if (listed) continue;
-        const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
-        const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
-        if (n == 0 || dst + n > p.cap) continue;
-        uint32_t* out = p.c_entries + dst;
-        uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr, [&](uint64_t k, uint32_t v) {
-          if (k < n) out[k] = v;
-        });
-        if (c != n) atomicOr(&p.ctl->status, 8ull);
-      }
-    }
-    __syncthreads();
   }
 }
 
@@ -1220,28 +588,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_fused(FusedArgs p) {
 
 }  // namespace
 
-void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
-                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
-  const uint32_t n = a_identity ? b->nrows : a->nrows;
-  if (n == 0) return;
-  // row mode unless the tiled mode is requested; an addend needs row mode
-  const bool row_mode = ctx->opt_spgemm_mode != 1;
-  if (d && !row_mode) throw Error(DVG_ERR_INVALID_ARG, "fused spgemm: an addend needs the row kernel");
-  auto kern = row_mode ? (a_identity ? k_spgemm_rowmode<true> : k_spgemm_rowmode<false>)
-                       : (a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>);
-  const int smem = int(row_mode ? sizeof(RowSmem) : sizeof(Smem));
-  DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  int per_sm = 0;
-  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
-  if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "fused spgemm: shared memory layout does not fit");
-  const uint64_t resident = uint64_t(per_sm) * ctx->num_sms;
-  // chunk rows: as large as possible (fewer look-back steps) while keeping
-  // about four chunks per resident CTA
-  uint32_t chunk_rows = kChunkMax;
-  while (chunk_rows > kSubRows && (uint64_t(n) + chunk_rows - 1) / chunk_rows < 4 * resident) chunk_rows >>= 1;
-  if (ctx->opt_chunk_rows > 0) chunk_rows = uint32_t(ctx->opt_chunk_rows);
-  const uint32_t nchunks = uint32_t((uint64_t(n) + chunk_rows - 1) / chunk_rows);
-  const size_t desc_bytes = size_t(nchunks) * sizeof(ChunkDesc);
+// Scratch for one single-pass product on the context: the chunk descriptors
+// (zeroed) and the ticket (zeroed).
+static void* chunk_scratch(dvg_context* ctx, size_t desc_bytes) {
   if (desc_bytes > ctx->tile_desc_cap) {
     if (ctx->d_tile_desc) dfree(ctx, ctx->d_tile_desc);
     ctx->d_tile_desc = nullptr;
@@ -1253,6 +602,50 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
   if (!ctx->d_ticket) ctx->d_ticket = static_cast<unsigned*>(dalloc(ctx, 256));
   DVG_CUDA(cudaMemsetAsync(ctx->d_tile_desc, 0, desc_bytes, ctx->stream));
   DVG_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(unsigned), ctx->stream));
+  return ctx->d_tile_desc;
+}
+
+void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
+                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
+  const uint32_t n = a_identity ? b->nrows : a->nrows;
+  if (n == 0) return;
+  // row mode unless the tiled mode is requested; an addend needs row mode
+  const bool row_mode = ctx->opt_spgemm_mode != 1;
+  if (d && !row_mode) throw Error(DVG_ERR_INVALID_ARG, "fused spgemm: an addend needs the row kernel");
+  if (row_mode) {
+    const RowLaunchShape shape = row_launch_shape(ctx, n, ctx->opt_chunk_rows, int(ctx->opt_row_slot));
+    RowLaunch L{};
+    L.a_rowmap = a_identity ? nullptr : a->rowmap;
+    L.a_entries = a_identity ? nullptr : a->entries;
+    L.a_identity = a_identity;
+    L.b_rowmap = b->rowmap;
+    L.b_entries = b->entries;
+    L.d_rowmap = d ? d->rowmap : nullptr;
+    L.d_entries = d ? d->entries : nullptr;
+    L.c_rowmap = c_rowmap;
+    L.c_entries = c_entries;
+    L.cap = cap;
+    L.nrows = n;
+    L.desc = chunk_scratch(ctx, shape.desc_bytes);
+    L.ticket = ctx->d_ticket;
+    L.ctl = ctx->d_ctl;
+    L.slot_variant = int(ctx->opt_row_slot);
+    launch_rowmode(ctx, L, shape);
+    return;
+  }
+  auto kern = a_identity ? k_spgemm_fused<true> : k_spgemm_fused<false>;
+  const int smem = int(sizeof(Smem));
+  DVG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+  if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "fused spgemm: shared memory layout does not fit");
+  const uint64_t resident = uint64_t(per_sm) * ctx->num_sms;
+  // chunk rows: as large as possible (fewer look-back steps) while keeping
+  // about four chunks per resident CTA
+  uint32_t chunk_rows = kChunkMax;
+  while (chunk_rows > kSubRows && (uint64_t(n) + chunk_rows - 1) / chunk_rows < 4 * resident) chunk_rows >>= 1;
+  if (ctx->opt_chunk_rows > 0) chunk_rows = uint32_t(ctx->opt_chunk_rows);
+  const uint32_t nchunks = uint32_t((uint64_t(n) + chunk_rows - 1) / chunk_rows);
   FusedArgs p{};
   p.a_rowmap = a_identity ? nullptr : a->rowmap;
   p.a_entries = a_identity ? nullptr : a->entries;
@@ -1261,16 +654,13 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
   p.c_rowmap = c_rowmap;
   p.c_entries = c_entries;
   p.cap = cap;
-  p.desc = static_cast<ChunkDesc*>(ctx->d_tile_desc);
+  p.desc = static_cast<ChunkDesc*>(chunk_scratch(ctx, size_t(nchunks) * sizeof(ChunkDesc)));
   p.ticket = ctx->d_ticket;
   p.ctl = ctx->d_ctl;
   p.nrows = n;
   p.chunk_rows = chunk_rows;
   p.nchunks = nchunks;
-  p.row_mode = row_mode ? 1u : 0u;
-  p.d_rowmap = d ? d->rowmap : nullptr;
-  p.d_entries = d ? d->entries : nullptr;
-  if (row_mode) ctx->stats.spgemm_light++;
+  p.row_mode = 0;
   const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
   kern<<<grid, kThreads, smem, ctx->stream>>>(p);
   DVG_CUDA(cudaGetLastError());

@@ -1,0 +1,391 @@
+// dvg_spgemm_rows.cu -- single-pass range SpGEMM, one C row per thread:
+// C = A B or C = D + A B (D a matrix of C's shape, or the identity).
+//
+// Same result as the reference's symbolic + numeric SpGEMM
+// (include/diverg/range_sparse.hpp:1132-1442 in cartoonist/diverg, dispatched
+// by range_spgemm :2215-2281) followed, for the sums, by range_spadd
+// (:112-357) on canonical operands: row r of C is the union of D's row r and
+// of all ranges of B rows s..f for every range [s,f] of A's row r, emitted as
+// sorted maximal runs.
+//
+// For the products of an index build the rows of C are a handful of runs,
+// however wide: the union is accumulated as a sorted list of disjoint,
+// non-adjacent runs -- exactly the canonical output -- held in the thread's
+// output slot in shared memory.  A range that overlaps or touches the open run
+// (kept in registers) extends it; any other range first merges the open run
+// into the list (insert, or merge with the runs it overlaps or touches: start
+// <= hi + 1, as the reference's accumulators merge).  The cost is output
+// sensitive and independent of the row's column span.  The shared footprint
+// is small (the slots, the chunk's row counts and the warp path's window), so
+// most of the SM's L1 caches the B ranges the threads read: the lanes of a
+// warp take consecutive rows, whose B slices overlap, and neighbouring warps
+// cover neighbouring rows.
+//
+// The kernel is persistent: CTAs take chunks of consecutive rows from an
+// atomic ticket; a chunk's rows are counted (runs into the slots), rows whose
+// runs overflow the slot are deferred to a warp-cooperative bitvector path, a
+// warp-parallel decoupled look-back over the chunk order gives the chunk's
+// output offset, and the slots are written out.  No symbolic pass, no scan
+// kernel.  Look-back waits are bounded (a timeout is recorded on expiry).
+#include <algorithm>
+#include <mutex>
+
+#include "dvg_spgemm_common.cuh"
+
+namespace dvg {
+namespace {
+
+constexpr int kRowRowsMax = kChunkMax / kThreads;  // rows per thread at the largest chunk
+constexpr int kRowDirectWW = 192;  // warp path: 32-bit window words per warp (6,144 columns)
+
+template <int SLOT>
+struct RowSmem {
+  uint32_t slot[SLOT * kThreads];       // entry k of thread t at [k * kThreads + t]
+  uint32_t direct[2 * kRowDirectWW * kWarps];  // warp path: bits + reach per warp
+  uint32_t incl[kChunkMax];
+  uint32_t slow[kSlowMax];              // rows left to the warp-cooperative path
+  unsigned long long red[kWarps];
+  unsigned long long prefix;
+  uint32_t chunk;
+  uint32_t nslow;
+};
+
+// Accumulates row `row` of C into the thread's slot from entry `pos` on.
+// Returns false, leaving no trace in nnz, when the runs overflow the slot.
+template <bool A_ID, int SLOT>
+__device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
+                         unsigned long long& nnz) {
+  uint32_t* L = S.slot + threadIdx.x + size_t(pos) * kThreads;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
+  const uint32_t max_runs = (uint32_t(SLOT) - pos) >> 1;
+  uint64_t a0, a1;
+  if (A_ID) {
+    a0 = 0;
+    a1 = 1;
+  } else {
+    a0 = __ldg(p.a_rowmap + row) >> 1;
+    a1 = __ldg(p.a_rowmap + row + 1) >> 1;
+  }
+  uint32_t nr = 0;
+  // merges [x, y] into the list; false when it needs more runs than fit
+  auto merge = [&](uint32_t x, uint32_t y) -> bool {
+    uint32_t k = 0;
+    while (k < nr && uint64_t(L[(2 * k + 1) * kThreads]) + 1 < x) ++k;
+    if (k == nr || uint64_t(y) + 1 < L[2 * k * kThreads]) {
+      if (nr == max_runs) return false;
+      for (uint32_t m = nr; m > k; --m) {
+        L[2 * m * kThreads] = L[2 * (m - 1) * kThreads];
+        L[(2 * m + 1) * kThreads] = L[(2 * m - 1) * kThreads];
+      }
+      L[2 * k * kThreads] = x;
+      L[(2 * k + 1) * kThreads] = y;
+      ++nr;
+      return true;
+    }
+    uint32_t lo = min(L[2 * k * kThreads], x), hi = max(L[(2 * k + 1) * kThreads], y);
+    uint32_t m = k + 1;
+    while (m < nr && uint64_t(hi) + 1 >= L[2 * m * kThreads]) {
+      hi = max(hi, L[(2 * m + 1) * kThreads]);
+      ++m;
+    }
+    L[2 * k * kThreads] = lo;
+    L[(2 * k + 1) * kThreads] = hi;
+    const uint32_t gone = m - k - 1;
+    if (gone) {
+      for (uint32_t q = m; q < nr; ++q) {
+        L[2 * (q - gone) * kThreads] = L[2 * q * kThreads];
+        L[(2 * (q - gone) + 1) * kThreads] = L[(2 * q + 1) * kThreads];
+      }
+      nr -= gone;
+    }
+    return true;
+  };
+  bool any = false;
+  uint32_t run_lo = 0, run_hi = 0;
+  // one input range: extend the open run, or merge the open run and open anew
+  auto take = [&](uint2 b) -> bool {
+    if (b.y < b.x) return true;
+    if (!any) {
+      any = true;
+      run_lo = b.x;
+      run_hi = b.y;
+      return true;
+    }
+    if (uint64_t(b.x) <= uint64_t(run_hi) + 1 && uint64_t(b.y) + 1 >= run_lo) {
+      run_lo = min(run_lo, b.x);
+      run_hi = max(run_hi, b.y);
+      return true;
+    }
+    if (!merge(run_lo, run_hi)) return false;
+    run_lo = b.x;
+    run_hi = b.y;
+    return true;
+  };
+  if (p.d_identity) {
+    take(make_uint2(uint32_t(row), uint32_t(row)));
+  } else if (p.d_rowmap) {
+    const uint64_t d0 = __ldg(p.d_rowmap + row) >> 1, d1 = __ldg(p.d_rowmap + row + 1) >> 1;
+    for (uint64_t t = d0; t < d1; ++t)
+      if (!take(load_range(p.d_entries, t))) return false;
+  }
+  for (uint64_t k = a0; k < a1; ++k) {
+    const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
+    if (ar.y < ar.x) continue;
+    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    for (uint64_t t = t0; t < t1; ++t)
+      if (!take(load_range(p.b_entries, t))) return false;
+  }
+  if (any && !merge(run_lo, run_hi)) return false;
+  uint64_t n = 0;
+  for (uint32_t k = 0; k < nr; ++k) n += uint64_t(L[(2 * k + 1) * kThreads]) - L[2 * k * kThreads] + 1;
+  count = 2 * nr;
+  nnz += n;
+  return true;
+}
+
+// The row kernel.  With rpt = ceil(chunk_rows / kThreads) rows per thread,
+// thread (warp, lane) owns chunk rows (warp * rpt + u) * 32 + lane, u < rpt:
+// the lanes of a warp take consecutive rows.
+template <bool A_ID, int SLOT>
+__global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RowSmem<SLOT>& S = *reinterpret_cast<RowSmem<SLOT>*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* dbits = S.direct + size_t(warp) * 2 * kRowDirectWW;
+  uint32_t* dreach = dbits + kRowDirectWW;
+  const uint32_t rpt = (p.chunk_rows + kThreads - 1) / kThreads;  // 1..kRowRowsMax
+  while (true) {
+    if (tid == 0) {
+      // a planned build stops at the first step whose output is unusable
+      const bool stop = p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
+      S.chunk = stop ? 0xffffffffu : atomicAdd(p.ticket, 1u);
+      S.nslow = 0;
+    }
+    __syncthreads();
+    const uint32_t t = S.chunk;
+    if (t >= p.nchunks) break;
+    const uint32_t c0row = t * p.chunk_rows;
+    const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
+    unsigned long long nnz_acc = 0;
+    uint32_t fast_mask = 0, pos = 0;
+    // rows that miss the slot wait for the warp-cooperative pass below, so
+    // one wide row never holds a whole chunk behind a single thread
+#pragma unroll
+    for (int u = 0; u < kRowRowsMax; ++u) {
+      if (uint32_t(u) >= rpt) break;
+      const uint32_t r = (warp * rpt + u) * 32 + lane;
+      if (r < crows) {
+        uint32_t cnt = 0;
+        if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, pos, cnt, nnz_acc)) {
+          fast_mask |= 1u << u;
+          pos += cnt;
+        } else {
+          const uint32_t i = atomicAdd(&S.nslow, 1u);
+          if (i < uint32_t(kSlowMax)) {
+            S.slow[i] = r;
+          } else {
+            cnt = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
+          }
+          atomicAdd(&p.ctl->slow_rows, 1ull);
+        }
+        S.incl[r] = cnt;
+      }
+    }
+    __syncthreads();
+    const uint32_t nslow = min(S.nslow, uint32_t(kSlowMax));
+    for (uint32_t i = warp; i < nslow; i += kWarps) {
+      const uint32_t r = S.slow[i];
+      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
+                                    [](uint64_t, uint32_t) {}, kRowDirectWW);
+      if (lane == 0) S.incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+    }
+    __syncthreads();
+    // chunk prefix over the row counts (kRowRowsMax consecutive rows per thread)
+    {
+      uint32_t loc[kRowRowsMax];
+      uint64_t s = 0;
+#pragma unroll
+      for (int k = 0; k < kRowRowsMax; ++k) {
+        const uint32_t r = tid * kRowRowsMax + k;
+        s += r < crows ? S.incl[r] : 0u;
+        loc[k] = uint32_t(s);
+      }
+      uint64_t inc = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint64_t u = __shfl_up_sync(kFullMask, inc, o);
+        if (lane >= o) inc += u;
+      }
+      if (lane == 31) S.red[warp] = inc;
+      __syncthreads();
+      uint64_t wpre = 0;
+      for (int i = 0; i < warp; ++i) wpre += S.red[i];
+      const uint64_t excl = wpre + inc - s;
+      if (excl + s > 0xffffffffull) raise_flag(p, &p.ctl->status, 16ull);
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kRowRowsMax; ++k) {
+        const uint32_t r = tid * kRowRowsMax + k;
+        if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
+      }
+    }
+    // chunk nnz
+    unsigned long long v = nnz_acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+    if (lane == 0) S.red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long chunk_nnz = 0;
+      for (int i = 0; i < kWarps; ++i) chunk_nnz += S.red[i];
+      const unsigned long long chunk_cnt = S.incl[crows - 1];
+      unsigned long long pre, pre_nnz;
+      lookback_warp(p, t, chunk_cnt, chunk_nnz, pre, pre_nnz);
+      if (lane == 0) {
+        S.prefix = pre;
+        if (t == p.nchunks - 1) {
+          p.ctl->total = pre + chunk_cnt;
+          p.ctl->nnz = pre_nnz + chunk_nnz;
+          if (pre + chunk_cnt > p.cap) raise_flag(p, &p.ctl->overflow, pre + chunk_cnt);
+        }
+      }
+    }
+    __syncthreads();
+    const unsigned long long prefix = S.prefix;
+    for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
+    if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
+    pos = 0;
+#pragma unroll
+    for (int u = 0; u < kRowRowsMax; ++u) {
+      if (uint32_t(u) >= rpt) break;
+      const uint32_t r = (warp * rpt + u) * 32 + lane;
+      if (r >= crows) continue;
+      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+      const bool fast = (fast_mask >> u) & 1u;
+      if (n && dst + n > p.cap) {
+        raise_flag(p, &p.ctl->overflow, 1ull);
+      } else if (fast) {
+        for (uint32_t k = 0; k < n; ++k) p.c_entries[dst + k] = S.slot[(pos + k) * kThreads + tid];
+      }
+      if (fast) pos += n;
+    }
+    // rows that missed the slot: the listed ones by warps, any overflow of
+    // the list by its own thread
+    for (uint32_t i = warp; i < nslow; i += kWarps) {
+      const uint32_t r = S.slow[i];
+      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+      if (n == 0 || dst + n > p.cap) continue;
+      uint32_t* out = p.c_entries + dst;
+      bool bad = false;
+      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
+                                    [&](uint64_t k, uint32_t v) {
+                                      if (k < n) out[k] = v;
+                                      else bad = true;
+                                    },
+                                    kRowDirectWW);
+      if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+    }
+    if (S.nslow > uint32_t(kSlowMax)) {
+#pragma unroll
+      for (int u = 0; u < kRowRowsMax; ++u) {
+        if (uint32_t(u) >= rpt) break;
+        const uint32_t r = (warp * rpt + u) * 32 + lane;
+        if (r >= crows || ((fast_mask >> u) & 1u)) continue;
+        bool listed = false;
+        for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
+        if (listed) continue;
+        const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
+        const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
+        if (n == 0 || dst + n > p.cap) continue;
+        uint32_t* out = p.c_entries + dst;
+        uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr, [&](uint64_t k, uint32_t v) {
+          if (k < n) out[k] = v;
+        });
+        if (c != n) raise_flag(p, &p.ctl->status, 8ull);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <bool A_ID, int SLOT>
+struct RowKernel {
+  static void* get() { return reinterpret_cast<void*>(&k_spgemm_rowmode<A_ID, SLOT>); }
+  static constexpr int smem() { return int(sizeof(RowSmem<SLOT>)); }
+};
+
+}  // namespace
+
+int row_slot_entries(int variant) {
+  static const int kSlots[] = {16, 24, 32};
+  return kSlots[std::min(std::max(variant, 0), 2)];
+}
+
+RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_rows_opt, int slot_variant) {
+  const int v = std::min(std::max(slot_variant, 0), 2);
+  // occupancy is a property of the kernel: queried once per context
+  if (ctx->row_resident[v] == 0) {
+    void* kern[3] = {RowKernel<false, 16>::get(), RowKernel<false, 24>::get(), RowKernel<false, 32>::get()};
+    void* kern_id[3] = {RowKernel<true, 16>::get(), RowKernel<true, 24>::get(), RowKernel<true, 32>::get()};
+    const int smem[3] = {RowKernel<false, 16>::smem(), RowKernel<false, 24>::smem(), RowKernel<false, 32>::smem()};
+    for (void* k : {kern[v], kern_id[v]})
+      DVG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem[v]));
+    int per_sm = 0;
+    DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern[v], kThreads, smem[v]));
+    if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "row spgemm: shared memory layout does not fit");
+    ctx->row_resident[v] = uint32_t(per_sm) * uint32_t(ctx->num_sms);
+  }
+  RowLaunchShape s{};
+  s.resident = ctx->row_resident[v];
+  // chunk rows: as large as possible (fewer look-back steps) while keeping
+  // about four chunks per resident CTA
+  uint32_t chunk_rows = kChunkMax;
+  while (chunk_rows > 64 && (uint64_t(nrows) + chunk_rows - 1) / chunk_rows < 4ull * s.resident) chunk_rows >>= 1;
+  if (chunk_rows_opt > 0) chunk_rows = uint32_t(std::min<int64_t>(chunk_rows_opt, kChunkMax));
+  s.chunk_rows = chunk_rows;
+  s.nchunks = uint32_t((uint64_t(nrows) + chunk_rows - 1) / chunk_rows);
+  s.grid = uint32_t(std::min<uint64_t>(s.nchunks, s.resident));
+  s.desc_bytes = size_t(s.nchunks) * sizeof(ChunkDesc);
+  return s;
+}
+
+void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& s) {
+  if (L.nrows == 0) return;
+  const int v = std::min(std::max(L.slot_variant, 0), 2);
+  FusedArgs p{};
+  p.a_rowmap = L.a_identity ? nullptr : L.a_rowmap;
+  p.a_entries = L.a_identity ? nullptr : L.a_entries;
+  p.b_rowmap = L.b_rowmap;
+  p.b_entries = L.b_entries;
+  p.c_rowmap = L.c_rowmap;
+  p.c_entries = L.c_entries;
+  p.cap = L.cap;
+  p.desc = static_cast<ChunkDesc*>(L.desc);
+  p.ticket = L.ticket;
+  p.ctl = L.ctl;
+  p.nrows = L.nrows;
+  p.chunk_rows = s.chunk_rows;
+  p.nchunks = s.nchunks;
+  p.row_mode = 1;
+  p.d_rowmap = L.d_identity ? nullptr : L.d_rowmap;
+  p.d_entries = L.d_identity ? nullptr : L.d_entries;
+  p.d_identity = L.d_identity ? 1u : 0u;
+  p.abort = L.abort;
+  const int smem[3] = {RowKernel<false, 16>::smem(), RowKernel<false, 24>::smem(), RowKernel<false, 32>::smem()};
+  const dim3 grid(s.grid), block(kThreads);
+  if (L.a_identity) {
+    if (v == 0) k_spgemm_rowmode<true, 16><<<grid, block, smem[v], ctx->stream>>>(p);
+    else if (v == 1) k_spgemm_rowmode<true, 24><<<grid, block, smem[v], ctx->stream>>>(p);
+    else k_spgemm_rowmode<true, 32><<<grid, block, smem[v], ctx->stream>>>(p);
+  } else {
+    if (v == 0) k_spgemm_rowmode<false, 16><<<grid, block, smem[v], ctx->stream>>>(p);
+    else if (v == 1) k_spgemm_rowmode<false, 24><<<grid, block, smem[v], ctx->stream>>>(p);
+    else k_spgemm_rowmode<false, 32><<<grid, block, smem[v], ctx->stream>>>(p);
+  }
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+  ctx->stats.spgemm_light++;
+}
+
+}  // namespace dvg

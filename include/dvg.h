@@ -68,6 +68,8 @@ typedef struct dvg_stats {
   uint64_t host_alloc_ns;       /* host time spent in device allocation calls */
   uint64_t host_sync_ns;        /* host time spent waiting on stream synchronisation */
   uint64_t spgemm_fused_adds;   /* products computed as D + A B in one pass */
+  uint64_t graph_launches;      /* CUDA graphs launched (batched builds) */
+  uint64_t autotune_builds;     /* planned builds run by the autotuner */
 } dvg_stats;
 
 /* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /
@@ -91,7 +93,15 @@ dvg_status dvg_synchronize(dvg_context* ctx);
  * to 2048), "spgemm_mode" (fused path: 0 = automatic, 1 = tile-staged rows,
  * 2 = a thread per row), "dindex_schedule" (0 = sum of powers of A, the
  * default; 1 = the reference's squaring of A + I; both give the same index),
- * "timing" (1 = time kernels with CUDA events into dvg_stats). */
+ * "planned_build" (1 = index builds run as a planned sequence of products with
+ * pre-allocated buffers and no host round trip between them, the default; 0 =
+ * one read-back per product), "plan_growth" (planned builds: the entry
+ * capacity of every step as a percentage of the input's entries, 300 by
+ * default and adapted after each build; a step that outgrows it makes the
+ * build re-run on the read-back path), "row_slot" (thread-per-row kernel: run-list
+ * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "timing" (1 =
+ * time kernels with CUDA events into dvg_stats).  Every setting gives the
+ * same results. */
 dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value);
 /* Device memory freed by the context's operations is kept for reuse; this
  * returns all of it to the CUDA allocator. */

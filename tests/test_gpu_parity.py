@@ -268,6 +268,51 @@ def test_index_fused_sums_on_fragmented_rows(ctx, window, chunk_rows):
     assert st["spgemm_fused_adds"] > 0 and st["spgemm_slow_rows"] > 2048
 
 
+@pytest.mark.parametrize("row_slot,chunk_rows", [(0, 0), (1, 512), (2, 1024), (0, 1056), (2, 2048), (1, 96)])
+@pytest.mark.parametrize("window", [(100, 300), (0, 37), (1, 1), (64, 64)])
+def test_planned_build_matches_oracle_and_synchronised_path(ctx, window, row_slot, chunk_rows):
+    # planned builds (one launch per step, no read-back between them) across
+    # run-list widths and chunk shapes, against the oracle and the read-back path
+    set_plan(ctx, (0, 0, 0, 0), chunk_rows)
+    ctx.set_option("row_slot", row_slot)
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(60_000, seed=9))
+    want = orc.dindex(omat(a), *window, algo="hbv")
+    da = ctx.upload(a)
+    try:
+        ctx.reset_stats()
+        got = ctx.distance_index(da, *window).download()
+        st = ctx.stats()
+        assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
+        assert st["spgemm_reruns"] == 0 and st["host_syncs"] <= 3, st
+        ctx.set_option("planned_build", 0)
+        again = ctx.distance_index(da, *window).download()
+        assert_same(again, want.rowmap, want.entries, want.nnz, str(window))
+    finally:
+        ctx.set_option("planned_build", 1)
+        ctx.set_option("row_slot", 1)
+
+
+def test_planned_build_outgrowing_its_estimate_reruns_exactly(ctx):
+    # a capacity estimate of nothing: the first step overflows, the later
+    # steps stand down, and the build re-runs on the read-back path
+    set_plan(ctx, (0, 0, 0, 0))
+    a = gen.random_matrix(4000, 24000, seed=85)
+    want = orc.dindex(omat(a), 2, 6)
+    da = ctx.upload(a)
+    ctx.set_option("plan_growth", 0)
+    ctx.reset_stats()
+    got = ctx.distance_index(da, 2, 6).download()
+    st = ctx.stats()
+    assert_same(got, want.rowmap, want.entries, want.nnz)
+    assert st["spgemm_reruns"] >= 1
+    # the estimate has grown: the next build stays planned
+    ctx.reset_stats()
+    again = ctx.distance_index(da, 2, 6).download()
+    assert_same(again, want.rowmap, want.entries, want.nnz)
+    assert ctx.stats()["spgemm_reruns"] == 0
+    ctx.set_option("plan_growth", 300)
+
+
 def test_query_batch_matches_oracle(ctx):
     a, _ = gen.graph_adjacency(gen.small_graph_spec(50_000, seed=4))
     idx = orc.dindex(omat(a), 100, 300, algo="hbv")
