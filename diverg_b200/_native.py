@@ -80,6 +80,7 @@ DVG_SIGNATURES = {
     "dvg_range_spgemm": [_P, _P, _P, _PP],
     "dvg_range_power": [_P, _P, ctypes.c_uint, _PP],
     "dvg_create_distance_index": [_P, _P, ctypes.c_uint, ctypes.c_uint, _PP],
+    "dvg_batch_distance_index": [_P, _U32, _P, _P, _P, _P],
     "dvg_query_batch": [_P, _P, _P, _U64, _P],
     "dvg_query_batch_host": [_P, _P, _P, _U64, _P],
     "dvg_range_spgemm_noalloc": [_U32, _U32, _P, _P, _U64, _U32, _U32, _P, _P, _U64, _P, _P, _U64,

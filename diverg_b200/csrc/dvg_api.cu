@@ -31,9 +31,7 @@ dvg_status guarded(F&& f) {
   }
 }
 
-void require(bool ok, const char* msg) {
-  if (!ok) throw dvg::Error(DVG_ERR_INVALID_ARG, msg);
-}
+using dvg::require;
 
 struct Lock {
   dvg_context* ctx;
@@ -47,6 +45,10 @@ struct Lock {
 }  // namespace
 
 namespace dvg {
+
+void require(bool ok, const char* msg) {
+  if (!ok) throw Error(DVG_ERR_INVALID_ARG, msg);
+}
 
 void record_error(const std::string& msg) { g_last_error = msg; }
 
@@ -687,6 +689,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "plan_growth")) {
       require(value >= 0 && value <= 100000, "plan_growth is a percentage in [0, 100000]");
       ctx->plan_growth = double(value) / 100.0;
+    } else if (!std::strcmp(key, "autotune")) {
+      require(value == 0 || value == 1, "autotune must be 0 or 1");
+      ctx->opt_autotune = value;
     } else if (!std::strcmp(key, "row_slot")) {
       require(value >= 0 && value <= 2, "row_slot must be 0 (16 entries), 1 (24) or 2 (32)");
       ctx->opt_row_slot = value;
@@ -940,6 +945,24 @@ dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, uns
       throw;
     }
     *out = r;
+  });
+}
+
+dvg_status dvg_batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* const* graphs,
+                                    const unsigned* dmin, const unsigned* dmax, dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(ngraphs == 0 || (graphs && dmin && dmax && out), "null argument");
+    batch_distance_index(ctx, ngraphs, graphs, dmin, dmax, out);
+    try {
+      read_control(ctx);
+    } catch (...) {
+      for (uint32_t k = 0; k < ngraphs; ++k) {
+        free_matrix(ctx, out[k]);
+        out[k] = nullptr;
+      }
+      throw;
+    }
   });
 }
 

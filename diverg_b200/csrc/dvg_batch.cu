@@ -225,6 +225,18 @@ void batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* 
     }
     if (!cur.members.empty()) groups.push_back(std::move(cur));
   }
+  if (groups.empty()) {
+    try {
+      for (uint32_t k : alone) out[k] = create_distance_index(ctx, graphs[k], dmin[k], dmax[k]);
+    } catch (...) {
+      for (uint32_t k = 0; k < ngraphs; ++k) {
+        free_matrix(ctx, out[k]);
+        out[k] = nullptr;
+      }
+      throw;
+    }
+    return;
+  }
   auto cleanup = [&]() {
     for (auto& g : groups) {
       if (g.planned) release_build(ctx, g.pb);

@@ -102,6 +102,8 @@ struct Error : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char* what);
+// Throws DVG_ERR_INVALID_ARG with `msg` unless `ok`.
+void require(bool ok, const char* msg);
 // Sets the message dvg_last_error() returns on the calling thread.
 void record_error(const std::string& msg);
 #define DVG_CUDA(call) ::dvg::cuda_check((call), #call)

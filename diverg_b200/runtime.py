@@ -113,6 +113,19 @@ class Context:
         N.check(N.lib().dvg_create_distance_index(self.handle, a.handle, dmin, dmax, ctypes.byref(h)))
         return DeviceMatrix(self, h)
 
+    def batch_distance_index(self, graphs, windows):
+        """Indices of many independent graphs (DeviceMatrix list) with their
+        (dmin, dmax) windows, built in one pass (dvg_batch_distance_index)."""
+        n = len(graphs)
+        if len(windows) != n:
+            raise ValueError("one window per graph")
+        hs = (ctypes.c_void_p * max(n, 1))(*[g.handle for g in graphs])
+        lo = (ctypes.c_uint * max(n, 1))(*[int(w[0]) for w in windows])
+        hi = (ctypes.c_uint * max(n, 1))(*[int(w[1]) for w in windows])
+        outs = (ctypes.c_void_p * max(n, 1))()
+        N.check(N.lib().dvg_batch_distance_index(self.handle, n, hs, lo, hi, outs))
+        return [DeviceMatrix(self, ctypes.c_void_p(outs[k])) for k in range(n)]
+
     def query(self, index, pairs: np.ndarray) -> np.ndarray:
         """Host pairs (npairs x 2 uint32) -> host uint8 answers."""
         pairs = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)

@@ -99,7 +99,10 @@ dvg_status dvg_synchronize(dvg_context* ctx);
  * capacity of every step as a percentage of the input's entries, 300 by
  * default and adapted after each build; a step that outgrows it makes the
  * build re-run on the read-back path), "row_slot" (thread-per-row kernel: run-list
- * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "timing" (1 =
+ * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "autotune" (1 =
+ * batches time the row kernel's shapes once per window and size class and
+ * keep the fastest, the default; 0 = use "row_slot" and "chunk_rows"),
+ * "timing" (1 =
  * time kernels with CUDA events into dvg_stats).  Every setting gives the
  * same results. */
 dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value);
@@ -150,6 +153,18 @@ dvg_status dvg_range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k, dv
  * Requires dmin <= dmax, dmax != 0 and a square `ra`. */
 dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, unsigned dmin, unsigned dmax,
                                      dvg_matrix** out);
+
+/* Distance indices of `ngraphs` independent graphs in one pass (no
+ * counterpart in the reference, which builds one graph per call): out[k]
+ * receives exactly what dvg_create_distance_index(graphs[k], dmin[k],
+ * dmax[k]) gives.  Graphs with the same window are laid side by side as one
+ * block-diagonal matrix and built together; the block-diagonal assemblies and
+ * the builds of all windows are captured into one CUDA graph and launched
+ * once; the autotuner (option "autotune") picks the row kernel's shape on the
+ * first batch of each window and size class.  On failure no output is left
+ * allocated. */
+dvg_status dvg_batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* const* graphs,
+                                    const unsigned* dmin, const unsigned* dmax, dvg_matrix** out);
 
 /* ---- range SpGEMM without device allocation -------------------------------
  * No counterpart in the reference.  Some callers of this library cannot let it
