@@ -52,6 +52,14 @@ def parse_args():
                    help="wall seconds the CPU baseline sample should take")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", choices=["build", "batch", "spgemm", "serve"], default="build",
+                   help="build: the plain chromosome-scale index build (the headline); batch: 2,000 "
+                        "mixed-size graphs in one batched build vs back-to-back single builds; spgemm: "
+                        "range_spgemm / range_spadd alone on banded 2^24-row matrices; serve: the "
+                        "request loop under Poisson arrivals")
+    p.add_argument("--graphs", type=int, default=2000, help="batch: number of graphs")
+    p.add_argument("--rate", type=float, default=0.0, help="serve: arrivals per second (0: sweep)")
+    p.add_argument("--requests", type=int, default=2000, help="serve: requests per rate")
     return p.parse_args()
 
 
@@ -194,6 +202,134 @@ def config_dict(args, n_loci):
             "parallelism": f"{args.gpus} independent graph(s), one per GPU"}
 
 
+def run_spgemm_micro(args, ctx, stream, rank):
+    """range_spgemm and range_spadd alone on random banded matrices: n = 2^24,
+    band half-width 512, Poisson(4) ranges per row of geometric length
+    (mean 32), canonical, fixed seeds.  Device-resident operands; each timed
+    product is bracketed by CUDA events on the library's stream."""
+    import torch
+    from diverg_b200 import gen
+    n = 1 << 24
+    a = gen.banded(n, 512, 4.0, 32.0, seed=args.seed + 2 * rank)
+    b = gen.banded(n, 512, 4.0, 32.0, seed=args.seed + 2 * rank + 1)
+    da, db = ctx.upload(a), ctx.upload(b)
+    peak, peak_kind = peaks()
+    res = {}
+    for name, op in (("range_spgemm", ctx.spgemm), ("range_spadd", ctx.spadd)):
+        for mode in ((2, 1) if name == "range_spgemm" else (0,)):
+            ctx.set_option("spgemm_mode", mode)
+            for _ in range(args.warmup):
+                op(da, db).free()
+            ctx.set_option("timing", 1)
+            ctx.reset_stats()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            ranges = 0
+            for _ in range(args.steps):
+                c = op(da, db)
+                ranges = c.nentries // 2
+                c.free()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            ctx.synchronize()
+            st = ctx.stats()
+            ctx.set_option("timing", 0)
+            kernel_ns = (st["spgemm_symbolic_ns"] + st["spgemm_numeric_ns"] + st["scan_ns"] + st["spadd_ns"])
+            alg = st["alg_bytes"]
+            call_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+            kern_s = kernel_ns / 1e9 / args.steps
+            gbs = alg / args.steps / kern_s / 1e9
+            res[f"{name}" + ("" if name != "range_spgemm" else ("[row]" if mode == 2 else "[tiled]"))] = {
+                "kernel_ms": kern_s * 1e3, "call_ms": call_s * 1e3, "alg_bytes": alg / args.steps,
+                "achieved_gbs": gbs, "frac": gbs / peak, "output_ranges": ranges,
+                "output_ranges_per_s": ranges / kern_s}
+    ctx.set_option("spgemm_mode", 0)
+    da.free()
+    db.free()
+    best = max((v for k, v in res.items() if k.startswith("range_spgemm")), key=lambda v: v["achieved_gbs"])
+    return {"metric": "range_spgemm HBM GB/s", "value": best["achieved_gbs"], "unit": "GB/s",
+            "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "kernel microbenchmark: range_spgemm and range_spadd of two random banded "
+                                   "matrices", "n": n, "half_width": 512, "ranges_per_row": "Poisson(4)",
+                       "range_length": "geometric, mean 32", "seeds": [args.seed, args.seed + 1],
+                       "l2": "operands (0.7 GB each) larger than L2"},
+            "peak": peak, "peak_kind": peak_kind, "kernels": res}
+
+
+def cfg3_batch(args, rank):
+    """2,000 graphs of the small-graph generator (bubbles 1/100: 70 % SNP,
+    30 % indel of length 1..10), sizes log-normal (median 2e4, sigma 1.0)
+    clipped to [1e3, 1e6] bases, windows drawn from {[100,300], [200,500],
+    [400,600]}, graph k seeded seed + k."""
+    import numpy as np
+    from diverg_b200 import gen
+    rng = np.random.default_rng(args.seed + 1000 * rank)
+    sizes = np.clip(rng.lognormal(np.log(2e4), 1.0, args.graphs), 1e3, 1e6).astype(np.int64)
+    wins = [(100, 300), (200, 500), (400, 600)]
+    windows = [wins[int(i)] for i in rng.integers(0, 3, args.graphs)]
+    graphs = [gen.graph_adjacency(gen.small_graph_spec(int(n), seed=args.seed + 1000 * rank + k))[0]
+              for k, n in enumerate(sizes)]
+    return graphs, windows
+
+
+def run_batch(args, ctx, stream, rank):
+    import numpy as np
+    import torch
+    graphs, windows = cfg3_batch(args, rank)
+    dg = [ctx.upload(g) for g in graphs]
+    loci = sum(g.numRows() for g in graphs)
+    # plain: back-to-back single builds, each bracketed by events
+    for k in range(min(50, len(dg))):
+        ctx.distance_index(dg[k], *windows[k]).free()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in dg]
+    sizes_plain = []
+    torch.cuda.synchronize()
+    for k, (d, w) in enumerate(zip(dg, windows)):
+        evs[k][0].record(stream)
+        ix = ctx.distance_index(d, *w)
+        evs[k][1].record(stream)
+        sizes_plain.append((ix.nentries, ix.nnz))
+        ix.free()
+    torch.cuda.synchronize()
+    lat_plain = np.array([e0.elapsed_time(e1) for e0, e1 in evs])
+    plain_s = evs[0][0].elapsed_time(evs[-1][1]) / 1e3
+    # batched: warm-up (the first batch autotunes), then timed batches
+    ctx.reset_stats()
+    for _ in range(args.warmup):
+        for ix in ctx.batch_distance_index(dg, windows):
+            ix.free()
+    tuned = ctx.stats()["autotune_builds"]
+    ctx.reset_stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    same = True
+    for _ in range(args.steps):
+        outs = ctx.batch_distance_index(dg, windows)
+        same = same and all((o.nentries, o.nnz) == sp for o, sp in zip(outs, sizes_plain))
+        for o in outs:
+            o.free()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    st = ctx.stats()
+    batch_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    for d in dg:
+        d.free()
+    n = len(dg)
+    return {"metric": "batched index builds/s", "value": n / batch_s, "unit": "builds/s", "higher_is_better": True,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "batched index builds of mixed-size graphs", "graphs": n, "loci": int(loci),
+                       "sizes": "log-normal, median 2e4 bases, sigma 1.0, clipped [1e3, 1e6]",
+                       "windows": "uniform over [100,300], [200,500], [400,600]", "seed": args.seed},
+            "plain_builds_per_s": n / plain_s, "speedup_vs_plain": plain_s / batch_s,
+            "latency_ms": {"batch": batch_s * 1e3, "plain_p50": float(np.percentile(lat_plain, 50)),
+                           "plain_p99": float(np.percentile(lat_plain, 99)), "plain_total": plain_s * 1e3},
+            "graph_launches_per_batch": st["graph_launches"] / args.steps,
+            "kernel_launches_per_batch": st["kernel_launches"] / args.steps,
+            "autotune_builds": tuned, "sizes_match_plain": bool(same)}
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -202,6 +338,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload != "build":
+        run_other(args, rank, world, local)
         return
 
     import numpy as np
@@ -336,6 +475,36 @@ def main():
         print(json.dumps(line), flush=True)
 
     d_a.free()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_other(args, rank, world, local):
+    """The secondary workloads: one replica per rank, rank 0 prints its line."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from diverg_b200.runtime import Context
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    with ClockSampler([local]) as clocks:
+        if args.workload == "spgemm":
+            line = run_spgemm_micro(args, ctx, stream, rank)
+        elif args.workload == "batch":
+            line = run_batch(args, ctx, stream, rank)
+        else:
+            from diverg_b200 import serving
+            line = serving.bench_line(args, ctx, rank)
+    line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "clocks": clocks.summary(),
+                 "scaling": "weak", "vs_baseline": None})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
         dist.barrier()

@@ -588,6 +588,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_fused(FusedArgs p) {
 
 }  // namespace
 
+// Mean A range length above which the automatic mode stages tiles.
+constexpr double kWideRangeMean = 8.0;
+
 // Scratch for one single-pass product on the context: the chunk descriptors
 // (zeroed) and the ticket (zeroed).
 static void* chunk_scratch(dvg_context* ctx, size_t desc_bytes) {
@@ -609,8 +612,14 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
                          const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   if (n == 0) return;
-  // row mode unless the tiled mode is requested; an addend needs row mode
-  const bool row_mode = ctx->opt_spgemm_mode != 1;
+  // mode 1 forces the tile-staged kernel, mode 2 the row kernel; automatic
+  // (0) takes the tile-staged kernel when A's ranges are long on average (its
+  // block unions then replace most B-row visits) and the row kernel otherwise.
+  // An addend needs the row kernel.
+  bool row_mode = ctx->opt_spgemm_mode != 1;
+  if (ctx->opt_spgemm_mode == 0 && !a_identity && !d && a->nentries > 0 &&
+      double(a->nnz) > kWideRangeMean * double(a->nentries / 2))
+    row_mode = false;
   if (d && !row_mode) throw Error(DVG_ERR_INVALID_ARG, "fused spgemm: an addend needs the row kernel");
   if (row_mode) {
     const RowLaunchShape shape = row_launch_shape(ctx, n, ctx->opt_chunk_rows, int(ctx->opt_row_slot));

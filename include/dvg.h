@@ -90,8 +90,9 @@ dvg_status dvg_synchronize(dvg_context* ctx);
  * autotune, or 4/8/16/32 lanes per output row), "window_words" (two-pass path:
  * 0 = default, else 32-bit accumulator words per row group), "chunk_rows"
  * (fused path: 0 = automatic, else rows per output chunk, a multiple of 32 up
- * to 2048), "spgemm_mode" (fused path: 0 = automatic, 1 = tile-staged rows,
- * 2 = a thread per row), "dindex_schedule" (0 = sum of powers of A, the
+ * to 2048), "spgemm_mode" (fused path: 0 = automatic -- tile-staged when A's
+ * ranges average more than 8 columns, else a thread per row --, 1 =
+ * tile-staged rows, 2 = a thread per row), "dindex_schedule" (0 = sum of powers of A, the
  * default; 1 = the reference's squaring of A + I; both give the same index),
  * "planned_build" (1 = index builds run as a planned sequence of products with
  * pre-allocated buffers and no host round trip between them, the default; 0 =
