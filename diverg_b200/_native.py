@@ -53,6 +53,27 @@ class GraphStats(ctypes.Structure):
         "n_loci", "n_snp", "n_ins", "n_del", "n_sv", "n_alt_loci")]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_uint64),
+                ("max_batch_builds", ctypes.c_uint32), ("max_inflight_queries", ctypes.c_uint32)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("request", ctypes.c_uint64), ("status", ctypes.c_int32), ("kind", ctypes.c_uint32),
+                ("submit_ns", ctypes.c_uint64), ("start_ns", ctypes.c_uint64), ("done_ns", ctypes.c_uint64),
+                ("index_entries", ctypes.c_uint64), ("index_nnz", ctypes.c_uint64),
+                ("invalid_pairs", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "builds_submitted", "builds_done", "build_batches", "queries_submitted", "queries_done", "pairs_answered",
+        "resident_bytes", "peak_reserved_bytes", "hbm_budget_bytes")]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 # Every entry point of include/dvg.h with its argument types.
 _P, _U32, _U64, _I64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int64
 _PP = ctypes.POINTER(ctypes.c_void_p)
@@ -85,6 +106,15 @@ DVG_SIGNATURES = {
     "dvg_query_batch_host": [_P, _P, _P, _U64, _P],
     "dvg_range_spgemm_noalloc": [_U32, _U32, _P, _P, _U64, _U32, _U32, _P, _P, _U64, _P, _P, _U64,
                                  ctypes.POINTER(_U64), ctypes.POINTER(_U64), _P],
+    "dvg_server_create": [ctypes.POINTER(ServerConfig), _PP],
+    "dvg_server_destroy": [_P],
+    "dvg_server_submit_build": [_P, _U32, _P, _P, ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(_U64)],
+    "dvg_server_submit_query": [_P, _U64, _P, _U64, _P, ctypes.POINTER(_U64)],
+    "dvg_server_poll": [_P, ctypes.POINTER(Completion), _U32, ctypes.POINTER(_U32), _U32],
+    "dvg_server_index_info": [_P, _U64, ctypes.POINTER(_U32), ctypes.POINTER(_U64), ctypes.POINTER(_U64)],
+    "dvg_server_download": [_P, _U64, _P, _P],
+    "dvg_server_release": [_P, _U64],
+    "dvg_server_get_stats": [_P, ctypes.POINTER(ServerStats)],
 }
 
 GEN_SIGNATURES = {

@@ -751,26 +751,38 @@ static uint64_t count_nnz_host(const uint32_t* e, uint64_t n) {
   return c;
 }
 
+}  // extern "C"
+
+namespace dvg {
+dvg_matrix* upload_matrix(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* rowmap,
+                          const uint32_t* entries, uint64_t nnz) {
+  require(rowmap != nullptr, "null argument");
+  require(ncols <= 0xFFFFFFFEu, "ncols must be below 2^32 - 1");
+  const uint64_t ne = rowmap[nrows];
+  require(ne == 0 || entries, "null entries");
+  dvg_matrix* m = new_matrix(ctx, nrows, ncols, ne);
+  try {
+    DVG_CUDA(cudaMemcpyAsync(m->rowmap, rowmap, (size_t(nrows) + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (ne) DVG_CUDA(cudaMemcpyAsync(m->entries, entries, ne * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->stats.h2d_bytes += (uint64_t(nrows) + 1) * 8 + ne * 4;
+    validate_uploaded(ctx, m);
+    m->nnz = nnz ? nnz : count_nnz_host(entries, ne);
+  } catch (...) {
+    free_matrix(ctx, m);
+    throw;
+  }
+  return m;
+}
+}  // namespace dvg
+
+extern "C" {
+
 dvg_status dvg_matrix_upload(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* rowmap,
                              const uint32_t* entries, uint64_t nnz, dvg_matrix** out) {
   return guarded([&] {
     Lock lk(ctx);
-    require(out && rowmap, "null argument");
-    require(ncols <= 0xFFFFFFFEu, "ncols must be below 2^32 - 1");
-    const uint64_t ne = rowmap[nrows];
-    require(ne == 0 || entries, "null entries");
-    dvg_matrix* m = new_matrix(ctx, nrows, ncols, ne);
-    try {
-      DVG_CUDA(cudaMemcpyAsync(m->rowmap, rowmap, (size_t(nrows) + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-      if (ne) DVG_CUDA(cudaMemcpyAsync(m->entries, entries, ne * 4, cudaMemcpyHostToDevice, ctx->stream));
-      ctx->stats.h2d_bytes += (uint64_t(nrows) + 1) * 8 + ne * 4;
-      validate_uploaded(ctx, m);
-      m->nnz = nnz ? nnz : count_nnz_host(entries, ne);
-    } catch (...) {
-      free_matrix(ctx, m);
-      throw;
-    }
-    *out = m;
+    require(out != nullptr, "null argument");
+    *out = upload_matrix(ctx, nrows, ncols, rowmap, entries, nnz);
   });
 }
 

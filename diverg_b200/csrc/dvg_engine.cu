@@ -165,6 +165,26 @@ PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_ma
   return pb;
 }
 
+uint64_t predict_build_bytes(double growth, uint32_t n, uint64_t nentries, unsigned dlo, unsigned dup) {
+  const IndexPlan plan = plan_index(dlo, dup);
+  std::vector<int> last_use(plan.nslots, -1);
+  for (size_t i = 0; i < plan.steps.size(); ++i)
+    for (int s : {plan.steps[i].a, plan.steps[i].b, plan.steps[i].d})
+      if (s >= 0) last_use[s] = int(i);
+  int live = 0, max_live = 1;
+  for (size_t i = 0; i < plan.steps.size(); ++i) {
+    max_live = std::max(max_live, ++live);
+    for (int s : {plan.steps[i].a, plan.steps[i].b, plan.steps[i].d})
+      if (s > 0 && last_use[s] == int(i) && s != plan.out) --live;
+  }
+  const uint64_t input = 8ull * (uint64_t(n) + 1) + 4ull * nentries;
+  const uint64_t est = std::max<uint64_t>(uint64_t(growth * double(nentries)), 4ull * n) + 64;
+  const uint64_t slot = 8ull * (uint64_t(n) + 1) + entries_alloc_bytes(est);
+  const uint64_t scratch = plan.steps.size() * ((uint64_t(n) / 64 + 1) * 32 + 512);
+  // the input is held twice while a batch lays it out block-diagonally
+  return 2 * input + uint64_t(max_live) * slot + scratch;
+}
+
 void release_build(dvg_context* ctx, PlannedBuild& pb) {
   for (int s = 1; s < int(pb.rowmap.size()); ++s) {
     if (pb.live[s]) {

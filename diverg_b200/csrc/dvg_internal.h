@@ -135,7 +135,9 @@ void launch_narrow_rowmap(dvg_context* ctx, const uint64_t* src, uint32_t* dst, 
 void launch_rowmap_scan(dvg_context* ctx, uint64_t* rowmap, uint64_t n);
 void launch_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity, uint64_t* c_rowmap,
                   uint32_t* c_entries, bool fill);
-void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out);
+// Out-of-range pairs are counted into ctl->invalid (ctx->d_ctl when null).
+void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out,
+                  DeviceControl* ctl = nullptr);
 
 struct SpgemmPlan {
   int group_lanes;   // lanes per output row: 4, 8, 16 or 32
@@ -193,6 +195,13 @@ dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
 dvg_matrix* range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity);
 dvg_matrix* range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k);
 dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigned dlo, unsigned dup);
+// Host range-CRS -> device (H2D, validation with one read-back).
+dvg_matrix* upload_matrix(dvg_context* ctx, uint32_t nrows, uint32_t ncols, const uint64_t* rowmap,
+                          const uint32_t* entries, uint64_t nnz);
+// Device bytes a planned build of an n x n input with `nentries` entries is
+// expected to hold at its peak (input, every live step's buffers at `growth`
+// times the input's entries, scratch).
+uint64_t predict_build_bytes(double growth, uint32_t n, uint64_t nentries, unsigned dlo, unsigned dup);
 
 inline uint64_t matrix_bytes(const dvg_matrix* m) {
   return 8ull * (uint64_t(m->nrows) + 1) + 4ull * m->nentries;

@@ -362,11 +362,12 @@ void launch_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bo
   ctx->stats.kernel_launches++;
 }
 
-void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out) {
+void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out,
+                  DeviceControl* ctl) {
   if (npairs == 0) return;
   k_query<<<grid_for(ctx, npairs, kThreads, 16), kThreads, 0, ctx->stream>>>(
       idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint2*>(d_pairs), npairs, d_out,
-      ctx->d_ctl);
+      ctl ? ctl : ctx->d_ctl);
   DVG_CUDA(cudaGetLastError());
   ctx->stats.kernel_launches++;
 }

@@ -207,6 +207,71 @@ dvg_status dvg_query_batch(dvg_context* ctx, const dvg_matrix* index, const uint
 dvg_status dvg_query_batch_host(dvg_context* ctx, const dvg_matrix* index, const uint32_t* pairs, uint64_t npairs,
                                 uint8_t* out);
 
+/* ---- serving: a request loop over resident indices ------------------------
+ * No counterpart in the reference, which builds one index per call and
+ * answers one pair per call.  A server owns two contexts on one device: a
+ * build worker admits waiting builds in arrival order while their predicted
+ * device footprint fits the HBM budget next to the resident indices, and
+ * builds all admitted graphs as one batch (dvg_batch_distance_index); a query
+ * worker runs every query batch whose index is resident, up to
+ * max_inflight_queries at once, on its own stream, concurrently with the
+ * builds.  Requests that arrive while others are on the device join the next
+ * batch or take the next free query slot.  Buffers passed to a request must
+ * stay valid until its completion is polled; pinned host buffers are copied
+ * directly, other ones through staging. */
+typedef struct dvg_server dvg_server;
+
+typedef struct dvg_server_config {
+  int device;
+  uint64_t hbm_budget_bytes;     /* resident indices + builds in flight; 0: 80 % of free memory */
+  uint32_t max_batch_builds;     /* builds merged into one batch; 0: 64 */
+  uint32_t max_inflight_queries; /* query batches on the device at once; 0: 8 */
+} dvg_server_config;
+
+typedef struct dvg_completion {
+  uint64_t request;        /* id returned at submission */
+  int32_t status;          /* dvg_status of the request */
+  uint32_t kind;           /* 1: build, 2: query batch */
+  uint64_t submit_ns;      /* steady-clock times: submitted, started on the device, completed */
+  uint64_t start_ns;
+  uint64_t done_ns;
+  uint64_t index_entries;  /* builds: the index's entries and nnz */
+  uint64_t index_nnz;
+  uint64_t invalid_pairs;  /* query batches: pairs outside the index (answered 0) */
+} dvg_completion;
+
+typedef struct dvg_server_stats {
+  uint64_t builds_submitted;
+  uint64_t builds_done;
+  uint64_t build_batches;
+  uint64_t queries_submitted;
+  uint64_t queries_done;
+  uint64_t pairs_answered;
+  uint64_t resident_bytes;       /* indices held in HBM */
+  uint64_t peak_reserved_bytes;  /* most resident + predicted in-flight bytes seen */
+  uint64_t hbm_budget_bytes;
+} dvg_server_stats;
+
+dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out);
+/* Finishes every submitted request, then frees the server and its indices. */
+dvg_status dvg_server_destroy(dvg_server* s);
+/* Queues the index build of an n x n range-CRS graph (host arrays); the
+ * request id is also the id of the index it makes. */
+dvg_status dvg_server_submit_build(dvg_server* s, uint32_t n, const uint64_t* rowmap, const uint32_t* entries,
+                                   unsigned dmin, unsigned dmax, uint64_t* request);
+/* Queues a batch of (row, column) membership queries against index `index`
+ * (a build request id); answers[q] receives 0 or 1. */
+dvg_status dvg_server_submit_query(dvg_server* s, uint64_t index, const uint32_t* pairs, uint64_t npairs,
+                                   uint8_t* answers, uint64_t* request);
+/* Takes up to `max` completions, waiting up to wait_ms for the first. */
+dvg_status dvg_server_poll(dvg_server* s, dvg_completion* out, uint32_t max, uint32_t* n, uint32_t wait_ms);
+dvg_status dvg_server_index_info(dvg_server* s, uint64_t index, uint32_t* nrows, uint64_t* nentries, uint64_t* nnz);
+/* Copies a resident index to host arrays (sizes from dvg_server_index_info). */
+dvg_status dvg_server_download(dvg_server* s, uint64_t index, uint64_t* rowmap, uint32_t* entries);
+/* Drops a resident index once the query batches on it have finished. */
+dvg_status dvg_server_release(dvg_server* s, uint64_t index);
+dvg_status dvg_server_get_stats(dvg_server* s, dvg_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,111 @@
+"""The request loop (dvg_server_*): a build and a query batch give the same
+index and answers alone and inside a busy mix of other requests, and both
+match the oracle exactly; builds are admitted within the memory budget."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as orc
+from diverg_b200 import CRSMatrix, _native as N, gen
+from diverg_b200.serving import Server
+
+pytestmark = pytest.mark.gpu
+
+WINDOW = (200, 500)
+
+
+def omat(m):
+    return orc.OMat(m.numRows(), m.numCols(), m.rowmap.astype(np.uint64), m.entries, m.nnz())
+
+
+def same(a: CRSMatrix, b: CRSMatrix):
+    return (a.numRows() == b.numRows() and np.array_equal(a.rowmap.astype(np.uint64), b.rowmap.astype(np.uint64))
+            and np.array_equal(a.entries, b.entries) and a.nnz() == b.nnz())
+
+
+def graph(n, seed):
+    return gen.graph_adjacency(gen.small_graph_spec(n, seed=seed))[0]
+
+
+def test_results_are_the_same_alone_and_in_the_mix():
+    target = graph(40_000, seed=11)
+    pairs = gen.query_pairs(target, 200_000, 0.5, *WINDOW, seed=12)
+    want = orc.dindex(omat(target), *WINDOW, algo="hbv")
+    want_crs = CRSMatrix(want.ncols, want.entries, want.rowmap, want.nnz)
+    want_answers = orc.query(want, pairs)
+
+    with Server(device=0) as srv:  # alone
+        b = srv.submit_build(target, *WINDOW)
+        assert srv.wait([b])[0]["status"] == N.OK
+        ans_alone = np.zeros(len(pairs), np.uint8)
+        q = srv.submit_query(b, pairs, ans_alone)
+        assert srv.wait([q])[0]["status"] == N.OK
+        idx_alone = srv.download(b)
+
+    others = [graph(int(n), seed=100 + k) for k, n in enumerate(np.linspace(5_000, 120_000, 12))]
+    other_pairs = [gen.query_pairs(g, 50_000 + 10_000 * k, 0.5, *WINDOW, seed=200 + k) for k, g in enumerate(others)]
+    with Server(device=0, max_batch_builds=4, max_inflight_queries=4) as srv:  # in the mix
+        ids, bids = [], []
+        answers = []
+        for k, g in enumerate(others[:6]):
+            bids.append(srv.submit_build(g, *WINDOW))
+        for k in range(6):
+            a = np.zeros(len(other_pairs[k]), np.uint8)
+            answers.append(a)
+            ids.append(srv.submit_query(bids[k], other_pairs[k], a))
+        b = srv.submit_build(target, *WINDOW)
+        for k, g in enumerate(others[6:], start=6):
+            bids.append(srv.submit_build(g, *WINDOW))
+        ans_mix = np.zeros(len(pairs), np.uint8)
+        q = srv.submit_query(b, pairs, ans_mix)
+        for k in range(6, 12):
+            a = np.zeros(len(other_pairs[k]), np.uint8)
+            answers.append(a)
+            ids.append(srv.submit_query(bids[k], other_pairs[k], a))
+        done = srv.wait(ids + bids + [b, q])
+        assert all(c["status"] == N.OK for c in done)
+        idx_mix = srv.download(b)
+        st = srv.stats()
+        # the other requests are right too
+        for k in (0, 7, 11):
+            got = srv.download(bids[k])
+            assert np.array_equal(answers[k], orc.query(omat(got), other_pairs[k]))
+    assert st["queries_done"] == 13 and st["builds_done"] == 13 and st["build_batches"] >= 2
+    assert same(idx_alone, want_crs) and same(idx_mix, want_crs)
+    assert np.array_equal(ans_alone, want_answers) and np.array_equal(ans_mix, want_answers)
+
+
+def test_builds_are_admitted_within_the_budget():
+    budget = 64 << 20
+    graphs = [graph(20_000, seed=300 + k) for k in range(10)]
+    with Server(device=0, hbm_budget_bytes=budget) as srv:
+        bids = [srv.submit_build(g, *WINDOW) for g in graphs]
+        done = srv.wait(bids)
+        assert all(c["status"] == N.OK for c in done)
+        st = srv.stats()
+        assert st["peak_reserved_bytes"] <= budget
+        assert st["build_batches"] >= 2
+        for k in (0, 9):
+            want = orc.dindex(omat(graphs[k]), *WINDOW, algo="hbv")
+            assert same(srv.download(bids[k]), CRSMatrix(want.ncols, want.entries, want.rowmap, want.nnz))
+
+
+def test_oversized_builds_bad_pairs_and_released_indices_report_errors():
+    big = graph(100_000, seed=400)
+    small = graph(5_000, seed=401)
+    with Server(device=0, hbm_budget_bytes=1 << 20) as srv:
+        b = srv.submit_build(big, *WINDOW)
+        q = srv.submit_query(b, np.zeros((4, 2), np.uint32), np.zeros(4, np.uint8))
+        c = srv.wait([b, q])
+        assert c[0]["status"] == N.OOM and c[1]["status"] == N.OOM
+    with Server(device=0) as srv:
+        b = srv.submit_build(small, *WINDOW)
+        srv.wait([b])
+        pairs = np.array([[0, 0], [small.numRows(), 0], [1, small.numRows() + 5]], np.uint32)
+        ans = np.full(3, 7, np.uint8)
+        c = srv.wait([srv.submit_query(b, pairs, ans)])[0]
+        assert c["status"] == N.INVALID_ARG and c["invalid_pairs"] == 2 and list(ans[1:]) == [0, 0]
+        srv.release(b)
+        c = srv.wait([srv.submit_query(b, pairs[:1], ans[:1])])[0]
+        assert c["status"] == N.INVALID_ARG
+        with pytest.raises(N.DvgError):
+            srv.release(b)
