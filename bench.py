@@ -36,6 +36,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per C row of the row kernel, mean of the four
+# launches of profiles/k_spgemm_rowmode_index_1e7.md (ncu, 10,019,292-row
+# graph): traffic scales with the rows of the product
+ROWMODE_TRAFFIC_BYTES_PER_ROW = (482445568 + 322691584 + 325835776 + 326179072 +
+                                 136677376 + 129849600 + 134458880 + 128670720) / 4 / 10019292
 
 
 def parse_args():
@@ -440,7 +445,10 @@ def main():
     per_product_s = spgemm_ns / 1e9 / spgemm_calls
     achieved = per_product_bytes / per_product_s / 1e9 if per_product_s > 0 else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": ROWMODE_TRAFFIC_BYTES_PER_ROW * n_loci,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                  "profiles/k_spgemm_rowmode_index_1e7.md, scaled by rows",
                 "peak_kind": peak_kind,
                 "kernel": "k_spgemm_rowmode (single-pass range SpGEMM: counts, chunk look-back, runs)",
                 "alg_bytes_per_product": per_product_bytes, "products_per_build": st["spgemm_calls"] / args.steps}
