@@ -37,24 +37,41 @@ namespace {
 
 constexpr int kRowRowsMax = kChunkMax / kThreads;  // rows per thread at the largest chunk
 constexpr int kRowDirectWW = 192;  // warp path: 32-bit window words per warp (6,144 columns)
+constexpr int kAStage = 2048;      // A ranges of a chunk staged in shared memory
+
+// The chunk's A row pointers and (up to kAStage of) its A ranges, loaded with
+// coalesced reads before the rows are walked; the warp path's windows reuse
+// the space once the rows have been counted.
+struct AStage {
+  uint64_t arow[kChunkMax + 1];
+  uint2 aent[kAStage];
+};
+union RowScratch {
+  uint32_t direct[2 * kRowDirectWW * kWarps];  // warp path: bits + reach per warp
+  AStage a;
+};
 
 template <int SLOT>
 struct RowSmem {
   uint32_t slot[SLOT * kThreads];       // entry k of thread t at [k * kThreads + t]
-  uint32_t direct[2 * kRowDirectWW * kWarps];  // warp path: bits + reach per warp
+  RowScratch u;
   uint32_t incl[kChunkMax];
   uint32_t slow[kSlowMax];              // rows left to the warp-cooperative path
   unsigned long long red[kWarps];
+  unsigned long long red_nnz[kWarps];
   unsigned long long prefix;
-  uint32_t chunk;
+  uint32_t next;                        // the chunk taken for the next iteration
   uint32_t nslow;
 };
 
-// Accumulates row `row` of C into the thread's slot from entry `pos` on.
-// Returns false, leaving no trace in nnz, when the runs overflow the slot.
+// Accumulates chunk row r (C row `row`) into the thread's slot from entry
+// `pos` on.  A's row pointers come from the stage, its ranges from the stage
+// when they are among the chunk's first kAStage ranges (abase: the chunk's
+// first range, nst: the number staged).  Returns false, leaving no trace in
+// nnz, when the runs overflow the slot.
 template <bool A_ID, int SLOT>
-__device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uint32_t pos, uint32_t& count,
-                         unsigned long long& nnz) {
+__device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uint32_t r, uint64_t abase,
+                         uint32_t nst, uint32_t pos, uint32_t& count, unsigned long long& nnz) {
   uint32_t* L = S.slot + threadIdx.x + size_t(pos) * kThreads;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
   const uint32_t max_runs = (uint32_t(SLOT) - pos) >> 1;
   uint64_t a0, a1;
@@ -62,8 +79,23 @@ __device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uin
     a0 = 0;
     a1 = 1;
   } else {
-    a0 = __ldg(p.a_rowmap + row) >> 1;
-    a1 = __ldg(p.a_rowmap + row + 1) >> 1;
+    a0 = S.u.a.arow[r] >> 1;
+    a1 = S.u.a.arow[r + 1] >> 1;
+  }
+  auto a_range = [&](uint64_t k) -> uint2 {
+    if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
+    return k - abase < nst ? S.u.a.aent[k - abase] : load_range(p.a_entries, k);
+  };
+  // the first A range's B row pointers are requested before the addend is
+  // walked, so their latency overlaps it
+  uint2 ar0 = make_uint2(1, 0);
+  uint64_t tb0 = 0, tb1 = 0;
+  if (a0 < a1) {
+    ar0 = a_range(a0);
+    if (ar0.x <= ar0.y) {
+      tb0 = __ldg(p.b_rowmap + ar0.x) >> 1;
+      tb1 = __ldg(p.b_rowmap + uint64_t(ar0.y) + 1) >> 1;
+    }
   }
   uint32_t nr = 0;
   // merges [x, y] into the list; false when it needs more runs than fit
@@ -128,9 +160,13 @@ __device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uin
       if (!take(load_range(p.d_entries, t))) return false;
   }
   for (uint64_t k = a0; k < a1; ++k) {
-    const uint2 ar = A_ID ? make_uint2(uint32_t(row), uint32_t(row)) : load_range(p.a_entries, k);
-    if (ar.y < ar.x) continue;
-    const uint64_t t0 = __ldg(p.b_rowmap + ar.x) >> 1, t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    uint64_t t0 = tb0, t1 = tb1;
+    if (k != a0) {
+      const uint2 ar = a_range(k);
+      if (ar.y < ar.x) continue;
+      t0 = __ldg(p.b_rowmap + ar.x) >> 1;
+      t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    }
     for (uint64_t t = t0; t < t1; ++t)
       if (!take(load_range(p.b_entries, t))) return false;
   }
@@ -150,21 +186,35 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   RowSmem<SLOT>& S = *reinterpret_cast<RowSmem<SLOT>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  uint32_t* dbits = S.direct + size_t(warp) * 2 * kRowDirectWW;
+  uint32_t* dbits = S.u.direct + size_t(warp) * 2 * kRowDirectWW;
   uint32_t* dreach = dbits + kRowDirectWW;
   const uint32_t rpt = (p.chunk_rows + kThreads - 1) / kThreads;  // 1..kRowRowsMax
-  while (true) {
-    if (tid == 0) {
-      // a planned build stops at the first step whose output is unusable
-      const bool stop = p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
-      S.chunk = stop ? 0xffffffffu : atomicAdd(p.ticket, 1u);
-      S.nslow = 0;
-    }
-    __syncthreads();
-    const uint32_t t = S.chunk;
-    if (t >= p.nchunks) break;
+  // a planned build stops at the first step whose output is unusable
+  auto take_ticket = [&]() -> uint32_t {
+    const bool stop = p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
+    return stop ? 0xffffffffu : atomicAdd(p.ticket, 1u);
+  };
+  if (tid == 0) {
+    S.next = take_ticket();
+    S.nslow = 0;
+  }
+  __syncthreads();
+  uint32_t t = S.next;
+  while (t < p.nchunks) {
     const uint32_t c0row = t * p.chunk_rows;
     const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
+    // stage A's row pointers and ranges of the chunk (coalesced)
+    uint64_t abase = 0;
+    uint32_t nst = 0;
+    if (!A_ID) {
+      for (uint32_t r = tid; r <= crows; r += kThreads) S.u.a.arow[r] = __ldg(p.a_rowmap + uint64_t(c0row) + r);
+      __syncthreads();
+      abase = S.u.a.arow[0] >> 1;
+      const uint64_t nrange = (S.u.a.arow[crows] >> 1) - abase;
+      nst = nrange < uint64_t(kAStage) ? uint32_t(nrange) : uint32_t(kAStage);
+      for (uint32_t k = tid; k < nst; k += kThreads) S.u.a.aent[k] = load_range(p.a_entries, abase + k);
+      __syncthreads();
+    }
     unsigned long long nnz_acc = 0;
     uint32_t fast_mask = 0, pos = 0;
     // rows that miss the slot wait for the warp-cooperative pass below, so
@@ -175,7 +225,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       const uint32_t r = (warp * rpt + u) * 32 + lane;
       if (r < crows) {
         uint32_t cnt = 0;
-        if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, pos, cnt, nnz_acc)) {
+        if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, r, abase, nst, pos, cnt, nnz_acc)) {
           fast_mask |= 1u << u;
           pos += cnt;
         } else {
@@ -191,15 +241,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       }
     }
     __syncthreads();
-    const uint32_t nslow = min(S.nslow, uint32_t(kSlowMax));
-    for (uint32_t i = warp; i < nslow; i += kWarps) {
-      const uint32_t r = S.slow[i];
-      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
-                                    [](uint64_t, uint32_t) {}, kRowDirectWW);
-      if (lane == 0) S.incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+    // the stage is dead from here on: the warp path may use the space
+    const uint32_t nslow_all = S.nslow;
+    const uint32_t nslow = min(nslow_all, uint32_t(kSlowMax));
+    if (nslow) {
+      for (uint32_t i = warp; i < nslow; i += kWarps) {
+        const uint32_t r = S.slow[i];
+        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
+                                      [](uint64_t, uint32_t) {}, kRowDirectWW);
+        if (lane == 0) S.incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    // chunk prefix over the row counts (kRowRowsMax consecutive rows per thread)
+    // chunk prefix over the row counts (kRowRowsMax consecutive rows per
+    // thread: a thread rewrites only its own rows) and the chunk's nnz
     {
       uint32_t loc[kRowRowsMax];
       uint64_t s = 0;
@@ -210,33 +265,31 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         loc[k] = uint32_t(s);
       }
       uint64_t inc = s;
+      unsigned long long v = nnz_acc;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         uint64_t u = __shfl_up_sync(kFullMask, inc, o);
         if (lane >= o) inc += u;
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
       if (lane == 31) S.red[warp] = inc;
+      if (lane == 0) S.red_nnz[warp] = v;
       __syncthreads();
       uint64_t wpre = 0;
       for (int i = 0; i < warp; ++i) wpre += S.red[i];
       const uint64_t excl = wpre + inc - s;
       if (excl + s > 0xffffffffull) raise_flag(p, &p.ctl->status, 16ull);
-      __syncthreads();
 #pragma unroll
       for (int k = 0; k < kRowRowsMax; ++k) {
         const uint32_t r = tid * kRowRowsMax + k;
         if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
       }
     }
-    // chunk nnz
-    unsigned long long v = nnz_acc;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
-    if (lane == 0) S.red[warp] = v;
     __syncthreads();
     if (warp == 0) {
       unsigned long long chunk_nnz = 0;
-      for (int i = 0; i < kWarps; ++i) chunk_nnz += S.red[i];
+      for (int i = 0; i < kWarps; ++i) chunk_nnz += S.red_nnz[i];
       const unsigned long long chunk_cnt = S.incl[crows - 1];
       unsigned long long pre, pre_nnz;
       lookback_warp(p, t, chunk_cnt, chunk_nnz, pre, pre_nnz);
@@ -250,6 +303,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       }
     }
     __syncthreads();
+    // the next chunk is taken now; its counts start from zero
+    if (tid == 0) {
+      S.next = take_ticket();
+      S.nslow = 0;
+    }
     const unsigned long long prefix = S.prefix;
     for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
     if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
@@ -286,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
                                     kRowDirectWW);
       if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
     }
-    if (S.nslow > uint32_t(kSlowMax)) {
+    if (nslow_all > uint32_t(kSlowMax)) {
 #pragma unroll
       for (int u = 0; u < kRowRowsMax; ++u) {
         if (uint32_t(u) >= rpt) break;
@@ -306,6 +364,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       }
     }
     __syncthreads();
+    t = S.next;
   }
 }
 
