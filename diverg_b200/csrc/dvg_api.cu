@@ -212,9 +212,65 @@ static DeviceControl read_total(dvg_context* ctx, const uint64_t* rowmap_last, u
   return c;
 }
 
+// Mean A range length from which a product reads union levels of B.
+constexpr double kLevelMean = 4.0;
+
+// Union levels of b: level k row j = the union of b's rows j .. j + 2^k - 1,
+// built as U_k = U_(k-1) + S U_(k-1) (S: identity shifted by 2^(k-1) rows).
+// A union of two rows has at most their entries together, so the capacity is
+// exact.
+static std::vector<dvg_matrix*> build_levels(dvg_context* ctx, const dvg_matrix* b, uint32_t nlevels) {
+  std::vector<dvg_matrix*> lv;
+  try {
+    const dvg_matrix* prev = b;
+    for (uint32_t k = 1; k <= nlevels; ++k) {
+      const uint64_t cap = 2 * prev->nentries + 64;
+      dvg_matrix* c = new_matrix(ctx, b->nrows, b->ncols, cap);
+      lv.push_back(c);
+      DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
+      reset_control(ctx);
+      cudaEvent_t t0 = span_begin(ctx);
+      launch_row_shifted_sum(ctx, prev, 1u << (k - 1), c->rowmap, c->entries, cap);
+      span_end(ctx, t0, kSymbolic);
+      const DeviceControl ctl = read_control(ctx);
+      if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "union levels: chunk look-back wait expired");
+      if (ctl.overflow) throw Error(DVG_ERR_DEVICE, "union levels: capacity overflow");
+      c->nentries = ctl.total;
+      c->nnz = ctl.nnz;
+      ctx->stats.spgemm_levels++;
+      ctx->stats.alg_bytes += 2 * matrix_bytes(prev) + matrix_bytes(c);
+      prev = c;
+    }
+  } catch (...) {
+    for (dvg_matrix* m : lv) free_matrix(ctx, m);
+    throw;
+  }
+  return lv;
+}
+
 static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
                                       const dvg_matrix* d = nullptr) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
+  // long A ranges: walk union levels of B instead of every B row
+  std::vector<dvg_matrix*> levels;
+  struct LevelGuard {
+    dvg_context* ctx;
+    std::vector<dvg_matrix*>& lv;
+    ~LevelGuard() {
+      for (dvg_matrix* m : lv) free_matrix(ctx, m);
+    }
+  } level_guard{ctx, levels};
+  if (!a_identity && !d && ctx->opt_levels && ctx->opt_spgemm_mode != 1 && a->nentries > 0 && b->nrows > 0) {
+    const double mean = double(a->nnz) / double(a->nentries / 2);
+    // automatic mode stages tiles above kWideRangeMean (faster there than
+    // levels on the banded and power-of-(A+I) products measured); levels serve
+    // the ranges between, and every long range when the row kernel is forced
+    if (mean >= kLevelMean && (ctx->opt_spgemm_mode == 2 || mean <= 8.0)) {
+      uint32_t nlv = 1;
+      while (nlv < 12 && double(1u << (nlv + 1)) <= 2.0 * mean) ++nlv;
+      levels = build_levels(ctx, b, nlv);
+    }
+  }
   // speculative output capacity; an overflow is detected and re-run exactly
   const uint64_t a_ent = a_identity ? 2ull * n : a->nentries;
   uint64_t cap = std::max<uint64_t>({2 * a_ent, 2 * b->nentries, d ? 2 * d->nentries : 0, 4ull * n, 64});
@@ -225,7 +281,7 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
     for (int attempt = 0; attempt < 2; ++attempt) {
       reset_control(ctx);
       cudaEvent_t t0 = span_begin(ctx);
-      launch_spgemm_fused(ctx, a, a_identity, b, d, c->rowmap, c->entries, cap);
+      launch_spgemm_fused(ctx, a, a_identity, b, d, c->rowmap, c->entries, cap, levels.empty() ? nullptr : &levels);
       span_end(ctx, t0, kSymbolic);
       ctl = read_control(ctx);
       if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "range_spgemm: tile look-back wait expired");
@@ -692,6 +748,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "autotune")) {
       require(value == 0 || value == 1, "autotune must be 0 or 1");
       ctx->opt_autotune = value;
+    } else if (!std::strcmp(key, "spgemm_levels")) {
+      require(value == 0 || value == 1, "spgemm_levels must be 0 or 1");
+      ctx->opt_levels = value;
     } else if (!std::strcmp(key, "row_slot")) {
       require(value >= 0 && value <= 2, "row_slot must be 0 (16 entries), 1 (24) or 2 (32)");
       ctx->opt_row_slot = value;

@@ -95,6 +95,12 @@ PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_ma
 
 PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_matrix* a, int slot_variant,
                            int64_t chunk_rows) {
+  const uint64_t t_prep = now_ns();
+  struct PrepTimer {
+    dvg_context* ctx;
+    uint64_t t0;
+    ~PrepTimer() { ctx->stats.host_prepare_ns += now_ns() - t0; }
+  } prep_timer{ctx, t_prep};
   PlannedBuild pb;
   pb.plan = plan;
   pb.input = a;
@@ -131,7 +137,9 @@ PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_ma
   // keep the plan within 80 % of the memory the device (and this context's
   // cache) can give; a step that then overflows re-runs on the read-back path
   size_t free_b = 0, total_b = 0;
+  const uint64_t tm = now_ns();
   DVG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  ctx->stats.host_meminfo_ns += now_ns() - tm;
   const double avail = 0.8 * double(free_b + ctx->cached_bytes) / double(max_live) - 8.0 * (double(pb.n) + 1);
   if (avail < 4.0 * double(est)) est = std::max<uint64_t>(uint64_t(std::max(avail, 0.0) / 4.0), 4ull * pb.n + 64);
   try {
@@ -198,6 +206,12 @@ void release_build(dvg_context* ctx, PlannedBuild& pb) {
 }
 
 void launch_build(dvg_context* ctx, PlannedBuild& pb, bool timed) {
+  const uint64_t t_launch = now_ns();
+  struct LaunchTimer {
+    dvg_context* ctx;
+    uint64_t t0;
+    ~LaunchTimer() { ctx->stats.host_launch_ns += now_ns() - t0; }
+  } launch_timer{ctx, t_launch};
   DVG_CUDA(cudaMemsetAsync(pb.scratch, 0, pb.scratch_bytes, ctx->stream));
   ctx->stats.kernel_launches++;
   const auto& steps = pb.plan.steps;
@@ -220,6 +234,7 @@ void launch_build(dvg_context* ctx, PlannedBuild& pb, bool timed) {
     L.c_entries = pb.entries[st.c];
     L.cap = pb.cap[st.c];
     L.nrows = pb.n;
+    L.b_nrows = pb.n;
     L.desc = static_cast<char*>(pb.scratch) + pb.desc_stride * i;
     L.ticket = pb.tickets + i;
     L.ctl = pb.ctls + i;

@@ -70,6 +70,7 @@ struct dvg_context {
   int64_t opt_spgemm_mode = 0;        // fused SpGEMM: 0 automatic, 1 tiled, 2 light
   int64_t opt_dindex_schedule = 0;    // 0: sum of powers, 1: the reference's squaring
   int64_t opt_row_slot = 1;           // row kernel run-list width variant (0: 16, 1: 24, 2: 32 entries)
+  int64_t opt_levels = 1;             // products with long A ranges read union levels of B (row kernel)
   uint32_t row_resident[3] = {0, 0, 0};  // resident CTAs of the row kernel per variant
   int64_t opt_planned = 1;            // 1: index builds run planned (no host round trips)
   double plan_growth = 3.0;           // planned builds: entry capacity per step / input entries
@@ -155,8 +156,14 @@ void launch_spgemm(dvg_context* ctx, const SpgemmPlan& plan, const dvg_matrix* a
 // c_entries up to `cap` entries; the control block receives the total entry
 // count, the nnz and an overflow flag when total > cap.
 // C = A B, or C = D + A B when d is not null (row kernel only)
+// `levels` (row kernel only): union levels of b, level k + 1 at index k.
 void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
-                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap);
+                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap,
+                         const std::vector<dvg_matrix*>* levels = nullptr);
+// C = U + S U with S the identity shifted by `shift` rows (row j of C is the
+// union of U's rows j and j + shift): one union level from the previous one.
+void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shift, uint64_t* c_rowmap,
+                            uint32_t* c_entries, uint64_t cap);
 
 // Thread-per-row single-pass product (dvg_spgemm_rows.cu) on raw arrays:
 // C = A B, C = D + A B, or C = I + A B (d_identity); A may be the identity.
@@ -181,6 +188,12 @@ struct RowLaunch {
   DeviceControl* ctl = nullptr;
   unsigned long long* abort = nullptr;
   int slot_variant = 1;  // run-list entries per thread: 0 -> 16, 1 -> 24, 2 -> 32
+  uint32_t a_shift = 0;  // with a_identity: A's row r is column r + a_shift (empty past b_nrows)
+  uint32_t b_nrows = 0;
+  // union levels of B (level k: rows j .. j + 2^k - 1 of B), at most 12
+  uint32_t nlevels = 0;
+  const uint64_t* lv_rowmap[12] = {};
+  const uint32_t* lv_entries[12] = {};
 };
 struct RowLaunchShape {
   uint32_t resident, chunk_rows, nchunks, grid;

@@ -25,6 +25,7 @@ constexpr int kStageMax = 6144;   // output entries staged per chunk
 constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
 constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
 constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
+constexpr int kMaxLevels = 12;    // union levels of B (blocks of up to 4096 rows)
 constexpr unsigned long long kFlag = 1ull << 63;
 constexpr uint32_t kSpinLimit = 1u << 22;
 
@@ -57,7 +58,24 @@ struct FusedArgs {
   // planned builds: a word every step checks before it starts and sets when
   // its output is unusable (overflow, timeout, internal error); null otherwise
   unsigned long long* abort;
+  // row mode, A the identity: A's row r is column r + a_shift (empty past B's
+  // last row), so C = D + S B adds B shifted up by a_shift rows
+  uint32_t a_shift;
+  uint32_t b_nrows;
+  // row mode: union levels of B, level k (1..nlevels) row j = the union of B
+  // rows j .. j + 2^k - 1 (rows past B's end count as empty); an A range of
+  // 4 or more rows takes a couple of level rows instead of its B rows
+  uint32_t nlevels;
+  const uint64_t* lv_rowmap[kMaxLevels];
+  const uint32_t* lv_entries[kMaxLevels];
 };
+
+// Row `row` of the (shifted) identity: column row + a_shift, or an empty
+// range when that is past B's last row.
+__device__ __forceinline__ uint2 id_range(const FusedArgs& p, uint64_t row) {
+  const uint64_t c = row + p.a_shift;
+  return (p.a_shift && c >= p.b_nrows) ? make_uint2(1u, 0u) : make_uint2(uint32_t(c), uint32_t(c));
+}
 
 // Records an error bit in the control block field and, in a planned build,
 // stops the steps that follow.
@@ -122,7 +140,9 @@ __device__ uint64_t direct_row(const FusedArgs& p, bool a_identity, uint64_t row
   auto slice = [&](uint64_t ai, uint64_t& b0, uint64_t& b1) {
     uint32_t s, f;
     if (a_identity) {
-      s = f = uint32_t(row);
+      const uint2 r = id_range(p, row);
+      s = r.x;
+      f = r.y;
     } else {
       uint2 r = load_range(p.a_entries, ai >> 1);
       s = r.x;
@@ -313,7 +333,7 @@ __device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const F
     a1 = p.a_rowmap[row + 1] >> 1;
   }
   auto a_range = [&](uint64_t k) -> uint2 {
-    if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
+    if (A_ID) return id_range(p, row);
     return a_staged ? achunk[k] : load_range(p.a_entries, k);
   };
   uint64_t d0 = 0, d1 = 0;  // the addend's ranges of this row

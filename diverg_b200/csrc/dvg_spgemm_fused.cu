@@ -608,8 +608,35 @@ static void* chunk_scratch(dvg_context* ctx, size_t desc_bytes) {
   return ctx->d_tile_desc;
 }
 
+void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shift, uint64_t* c_rowmap,
+                            uint32_t* c_entries, uint64_t cap) {
+  if (u->nrows == 0) return;
+  // level rows gather many runs: unless set, a row per thread and the widest run list
+  const int64_t chunk_rows = ctx->opt_chunk_rows ? ctx->opt_chunk_rows : 512;
+  const int slot = ctx->opt_row_slot == 1 ? 2 : int(ctx->opt_row_slot);
+  const RowLaunchShape shape = row_launch_shape(ctx, u->nrows, chunk_rows, slot);
+  RowLaunch L{};
+  L.a_identity = true;
+  L.a_shift = shift;
+  L.b_rowmap = u->rowmap;
+  L.b_entries = u->entries;
+  L.b_nrows = u->nrows;
+  L.d_rowmap = u->rowmap;
+  L.d_entries = u->entries;
+  L.c_rowmap = c_rowmap;
+  L.c_entries = c_entries;
+  L.cap = cap;
+  L.nrows = u->nrows;
+  L.desc = chunk_scratch(ctx, shape.desc_bytes);
+  L.ticket = ctx->d_ticket;
+  L.ctl = ctx->d_ctl;
+  L.slot_variant = slot;
+  launch_rowmode(ctx, L, shape);
+}
+
 void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b,
-                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap) {
+                         const dvg_matrix* d, uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap,
+                         const std::vector<dvg_matrix*>* levels) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   if (n == 0) return;
   // mode 1 forces the tile-staged kernel, mode 2 the row kernel; automatic
@@ -617,18 +644,31 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
   // block unions then replace most B-row visits) and the row kernel otherwise.
   // An addend needs the row kernel.
   bool row_mode = ctx->opt_spgemm_mode != 1;
-  if (ctx->opt_spgemm_mode == 0 && !a_identity && !d && a->nentries > 0 &&
+  if (ctx->opt_spgemm_mode == 0 && !a_identity && !d && !(levels && !levels->empty()) && a->nentries > 0 &&
       double(a->nnz) > kWideRangeMean * double(a->nentries / 2))
     row_mode = false;
   if (d && !row_mode) throw Error(DVG_ERR_INVALID_ARG, "fused spgemm: an addend needs the row kernel");
   if (row_mode) {
-    const RowLaunchShape shape = row_launch_shape(ctx, n, ctx->opt_chunk_rows, int(ctx->opt_row_slot));
+    // products that read union levels (long A ranges) have rows of many runs:
+    // unless set, a row per thread and the widest run list
+    const bool wide = levels && !levels->empty();
+    const int64_t chunk_rows = ctx->opt_chunk_rows ? ctx->opt_chunk_rows : (wide ? 512 : 0);
+    const int slot = wide && ctx->opt_row_slot == 1 ? 2 : int(ctx->opt_row_slot);
+    const RowLaunchShape shape = row_launch_shape(ctx, n, chunk_rows, slot);
     RowLaunch L{};
     L.a_rowmap = a_identity ? nullptr : a->rowmap;
     L.a_entries = a_identity ? nullptr : a->entries;
     L.a_identity = a_identity;
     L.b_rowmap = b->rowmap;
     L.b_entries = b->entries;
+    L.b_nrows = b->nrows;
+    if (levels) {
+      L.nlevels = uint32_t(std::min<size_t>(levels->size(), 12));
+      for (uint32_t k = 0; k < L.nlevels; ++k) {
+        L.lv_rowmap[k] = (*levels)[k]->rowmap;
+        L.lv_entries[k] = (*levels)[k]->entries;
+      }
+    }
     L.d_rowmap = d ? d->rowmap : nullptr;
     L.d_entries = d ? d->entries : nullptr;
     L.c_rowmap = c_rowmap;
@@ -638,7 +678,7 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
     L.desc = chunk_scratch(ctx, shape.desc_bytes);
     L.ticket = ctx->d_ticket;
     L.ctl = ctx->d_ctl;
-    L.slot_variant = int(ctx->opt_row_slot);
+    L.slot_variant = slot;
     launch_rowmode(ctx, L, shape);
     return;
   }

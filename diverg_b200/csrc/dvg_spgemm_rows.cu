@@ -83,16 +83,18 @@ __device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uin
     a1 = S.u.a.arow[r + 1] >> 1;
   }
   auto a_range = [&](uint64_t k) -> uint2 {
-    if (A_ID) return make_uint2(uint32_t(row), uint32_t(row));
+    if (A_ID) return id_range(p, row);
     return k - abase < nst ? S.u.a.aent[k - abase] : load_range(p.a_entries, k);
   };
+  // an A range of at least 4 rows reads union levels when B has them
+  auto leveled = [&](uint2 ar) { return p.nlevels && ar.y >= ar.x && ar.y - ar.x >= 3u; };
   // the first A range's B row pointers are requested before the addend is
   // walked, so their latency overlaps it
   uint2 ar0 = make_uint2(1, 0);
   uint64_t tb0 = 0, tb1 = 0;
   if (a0 < a1) {
     ar0 = a_range(a0);
-    if (ar0.x <= ar0.y) {
+    if (ar0.x <= ar0.y && !leveled(ar0)) {
       tb0 = __ldg(p.b_rowmap + ar0.x) >> 1;
       tb1 = __ldg(p.b_rowmap + uint64_t(ar0.y) + 1) >> 1;
     }
@@ -160,10 +162,26 @@ __device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uin
       if (!take(load_range(p.d_entries, t))) return false;
   }
   for (uint64_t k = a0; k < a1; ++k) {
+    const uint2 ar = k == a0 ? ar0 : a_range(k);
+    if (ar.y < ar.x) continue;
+    if (leveled(ar)) {
+      // blocks of 2^lv rows from s, the last one ending at f (they may overlap)
+      const uint32_t len = ar.y - ar.x + 1;
+      const uint32_t lv = min(uint32_t(31 - __clz(len)), p.nlevels);
+      const uint32_t step = 1u << lv, last = ar.y - step + 1;
+      const uint64_t* __restrict__ lr = p.lv_rowmap[lv - 1];
+      const uint32_t* __restrict__ le = p.lv_entries[lv - 1];
+      for (uint32_t blk0 = ar.x;; blk0 += step) {
+        const uint32_t blk = min(blk0, last);
+        const uint64_t u0 = __ldg(lr + blk) >> 1, u1 = __ldg(lr + uint64_t(blk) + 1) >> 1;
+        for (uint64_t t = u0; t < u1; ++t)
+          if (!take(load_range(le, t))) return false;
+        if (blk == last) break;
+      }
+      continue;
+    }
     uint64_t t0 = tb0, t1 = tb1;
     if (k != a0) {
-      const uint2 ar = a_range(k);
-      if (ar.y < ar.x) continue;
       t0 = __ldg(p.b_rowmap + ar.x) >> 1;
       t1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
     }
@@ -431,6 +449,13 @@ void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& 
   p.d_entries = L.d_identity ? nullptr : L.d_entries;
   p.d_identity = L.d_identity ? 1u : 0u;
   p.abort = L.abort;
+  p.a_shift = L.a_identity ? L.a_shift : 0u;
+  p.b_nrows = L.b_nrows;
+  p.nlevels = L.nlevels;
+  for (uint32_t k = 0; k < L.nlevels && k < uint32_t(kMaxLevels); ++k) {
+    p.lv_rowmap[k] = L.lv_rowmap[k];
+    p.lv_entries[k] = L.lv_entries[k];
+  }
   const int smem[3] = {RowKernel<false, 16>::smem(), RowKernel<false, 24>::smem(), RowKernel<false, 32>::smem()};
   const dim3 grid(s.grid), block(kThreads);
   if (L.a_identity) {

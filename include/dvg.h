@@ -70,6 +70,10 @@ typedef struct dvg_stats {
   uint64_t spgemm_fused_adds;   /* products computed as D + A B in one pass */
   uint64_t graph_launches;      /* CUDA graphs launched (batched builds) */
   uint64_t autotune_builds;     /* planned builds run by the autotuner */
+  uint64_t spgemm_levels;       /* union levels of B built for long-range products */
+  uint64_t host_prepare_ns;     /* host time planning builds (buffers, shapes) */
+  uint64_t host_launch_ns;      /* host time issuing the planned builds' work */
+  uint64_t host_meminfo_ns;     /* host time querying free device memory */
 } dvg_stats;
 
 /* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /
@@ -100,7 +104,12 @@ dvg_status dvg_synchronize(dvg_context* ctx);
  * capacity of every step as a percentage of the input's entries, 300 by
  * default and adapted after each build; a step that outgrows it makes the
  * build re-run on the read-back path), "row_slot" (thread-per-row kernel: run-list
- * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "autotune" (1 =
+ * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "spgemm_levels"
+ * (1 = a thread-per-row product whose A ranges average 4 or more rows -- up
+ * to 8 in automatic mode, which stages tiles above that -- first builds union
+ * levels of B -- level k row j is the union of B's rows j .. j + 2^k - 1 --
+ * and reads a couple of level rows per A range instead of its B rows, the
+ * default; 0 = never), "autotune" (1 =
  * batches time the row kernel's shapes once per window and size class and
  * keep the fastest, the default; 0 = use "row_slot" and "chunk_rows"),
  * "timing" (1 =

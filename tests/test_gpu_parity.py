@@ -199,6 +199,22 @@ def test_fused_direct_tiles_and_capacity_rerun(ctx, chunk_rows):
     assert st["spgemm_reruns"] == 1
 
 
+@pytest.mark.parametrize("mean_len,hw", [(6.0, 64), (32.0, 512), (300.0, 4096)])
+@pytest.mark.parametrize("levels", [0, 1])
+def test_long_range_products_with_union_levels(ctx, mean_len, hw, levels):
+    # A ranges of many rows: the row kernel reads union levels of B (blocks of
+    # 2^k rows, several per range when a range is longer than the top level)
+    set_plan(ctx, (0, 0, 0, 2))
+    ctx.set_option("spgemm_levels", levels)
+    try:
+        a = gen.banded(40_000, hw, 3.0, mean_len, seed=91)
+        b = gen.banded(40_000, 256, 4.0, 8.0, seed=92)
+        st = spgemm_case(ctx, a, b)
+        assert (st["spgemm_levels"] > 0) == bool(levels)
+    finally:
+        ctx.set_option("spgemm_levels", 1)
+
+
 def test_algos_agree_on_cfg2_shape_sample(ctx):
     # the kernel microbenchmark shape (banded, half-width 512, Poisson(4)
     # ranges of geometric length 32) at 2^20 rows: both kernels and the oracle
