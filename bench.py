@@ -57,6 +57,8 @@ def parse_args():
                    help="wall seconds the CPU baseline sample should take")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                   help="a context option (dvg_set_option) for the run; repeatable")
     p.add_argument("--workload", choices=["build", "batch", "spgemm", "serve"], default="build",
                    help="build: the plain chromosome-scale index build (the headline); batch: 2,000 "
                         "mixed-size graphs in one batched build vs back-to-back single builds; spgemm: "
@@ -204,7 +206,8 @@ def config_dict(args, n_loci):
             "bubbles": "SNP 1/1000, indel 1/5000 (geometric mean 4, cap 50), 0.1% structural (100..2000)",
             "seed": args.seed, "index_types": "uint32 columns, uint64 rowmap",
             "l2": "inputs larger than L2 (A and every intermediate exceed 126 MB)",
-            "parallelism": f"{args.gpus} independent graph(s), one per GPU"}
+            "parallelism": f"{args.gpus} independent graph(s), one per GPU",
+            **({"options": list(args.set)} if args.set else {})}
 
 
 def run_spgemm_micro(args, ctx, stream, rank):
@@ -335,6 +338,12 @@ def run_batch(args, ctx, stream, rank):
             "autotune_builds": tuned, "sizes_match_plain": bool(same)}
 
 
+def apply_options(ctx, pairs):
+    for kv in pairs:
+        key, _, value = kv.partition("=")
+        ctx.set_option(key.strip(), int(value))
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -373,6 +382,7 @@ def main():
     a, gstats = graph(args.n_backbone, args.seed + rank)
     n_loci = a.numRows()
     ctx = Context(local)
+    apply_options(ctx, args.set)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     d_a = ctx.upload(a)
@@ -499,6 +509,7 @@ def run_other(args, rank, world, local):
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     ctx = Context(local)
+    apply_options(ctx, args.set)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     with ClockSampler([local]) as clocks:

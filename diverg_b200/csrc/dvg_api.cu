@@ -688,6 +688,7 @@ dvg_status dvg_shutdown(dvg_context* ctx) {
     if (ctx->d_pairs) dfree(ctx, ctx->d_pairs);
     if (ctx->d_answers) dfree(ctx, ctx->d_answers);
     if (ctx->d_tile_desc) dfree(ctx, ctx->d_tile_desc);
+    if (ctx->d_row_stage) dfree(ctx, ctx->d_row_stage);
     if (ctx->d_ticket) dfree(ctx, ctx->d_ticket);
     release_cached(ctx);
     DVG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -751,6 +752,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "spgemm_levels")) {
       require(value == 0 || value == 1, "spgemm_levels must be 0 or 1");
       ctx->opt_levels = value;
+    } else if (!std::strcmp(key, "row_stage")) {
+      require(value == 0 || value == 1, "row_stage must be 0 or 1");
+      ctx->opt_row_stage = value;
     } else if (!std::strcmp(key, "row_slot")) {
       require(value >= 0 && value <= 2, "row_slot must be 0 (16 entries), 1 (24) or 2 (32)");
       ctx->opt_row_slot = value;

@@ -148,6 +148,7 @@ PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_ma
     pb.tickets = reinterpret_cast<unsigned*>(base + tickets_off);
     pb.ctls = reinterpret_cast<DeviceControl*>(base + ctl_off);
     pb.abort = reinterpret_cast<unsigned long long*>(base + abort_off);
+    if (ctx->opt_row_stage) pb.stage = static_cast<uint32_t*>(dalloc(ctx, pb.shape.stage_bytes));
     for (size_t i = 0; i < nsteps; ++i) {
       const int c = plan.steps[i].c;
       pb.owner_step[c] = int(i);
@@ -188,7 +189,9 @@ uint64_t predict_build_bytes(double growth, uint32_t n, uint64_t nentries, unsig
   const uint64_t input = 8ull * (uint64_t(n) + 1) + 4ull * nentries;
   const uint64_t est = std::max<uint64_t>(uint64_t(growth * double(nentries)), 4ull * n) + 64;
   const uint64_t slot = 8ull * (uint64_t(n) + 1) + entries_alloc_bytes(est);
-  const uint64_t scratch = plan.steps.size() * ((uint64_t(n) / 64 + 1) * 32 + 512);
+  // chunk descriptors, and the row kernel's staging: two buffers of 17 words
+  // a chunk row per CTA, at most about 136 bytes a row
+  const uint64_t scratch = plan.steps.size() * ((uint64_t(n) / 64 + 1) * 32 + 512) + 136ull * n;
   // the input is held twice while a batch lays it out block-diagonally
   return 2 * input + uint64_t(max_live) * slot + scratch;
 }
@@ -203,6 +206,8 @@ void release_build(dvg_context* ctx, PlannedBuild& pb) {
   }
   if (pb.scratch) dfree(ctx, pb.scratch);
   pb.scratch = nullptr;
+  if (pb.stage) dfree(ctx, pb.stage);
+  pb.stage = nullptr;
 }
 
 void launch_build(dvg_context* ctx, PlannedBuild& pb, bool timed) {
@@ -239,6 +244,7 @@ void launch_build(dvg_context* ctx, PlannedBuild& pb, bool timed) {
     L.ticket = pb.tickets + i;
     L.ctl = pb.ctls + i;
     L.abort = pb.abort;
+    L.stage_buf = pb.stage;
     L.slot_variant = pb.slot_variant;
     cudaEvent_t t0 = timed ? span_begin(ctx) : nullptr;
     launch_rowmode(ctx, L, pb.shape);

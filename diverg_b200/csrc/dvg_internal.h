@@ -69,6 +69,9 @@ struct dvg_context {
   int64_t opt_chunk_rows = 0;         // fused SpGEMM look-back chunk rows (0: automatic)
   int64_t opt_spgemm_mode = 0;        // fused SpGEMM: 0 automatic, 1 tiled, 2 light
   int64_t opt_dindex_schedule = 0;    // 0: sum of powers, 1: the reference's squaring
+  int64_t opt_row_stage = 1;          // row kernel defers write-out through staging buffers
+  uint32_t* d_row_stage = nullptr;    // staging for single products
+  size_t row_stage_cap = 0;           // bytes
   int64_t opt_row_slot = 1;           // row kernel run-list width variant (0: 16, 1: 24, 2: 32 entries)
   int64_t opt_levels = 1;             // products with long A ranges read union levels of B (row kernel)
   uint32_t row_resident[3] = {0, 0, 0};  // resident CTAs of the row kernel per variant
@@ -194,10 +197,13 @@ struct RowLaunch {
   uint32_t nlevels = 0;
   const uint64_t* lv_rowmap[12] = {};
   const uint32_t* lv_entries[12] = {};
+  // staging for deferred write-out, RowLaunchShape::stage_bytes (null: off)
+  uint32_t* stage_buf = nullptr;
 };
 struct RowLaunchShape {
   uint32_t resident, chunk_rows, nchunks, grid;
   size_t desc_bytes;
+  size_t stage_bytes;  // staging buffers of the whole grid
 };
 RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_rows_opt, int slot_variant);
 void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& shape);
@@ -265,6 +271,7 @@ struct PlannedBuild {
   unsigned* tickets = nullptr;
   DeviceControl* ctls = nullptr;
   unsigned long long* abort = nullptr;
+  uint32_t* stage = nullptr;        // row kernel staging (shape.stage_bytes), shared by the steps
 };
 // Allocates every buffer of the plan for input `a` (no device work beyond
 // stream-ordered allocation).

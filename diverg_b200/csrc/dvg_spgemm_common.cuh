@@ -29,11 +29,13 @@ constexpr int kMaxLevels = 12;    // union levels of B (blocks of up to 4096 row
 constexpr unsigned long long kFlag = 1ull << 63;
 constexpr uint32_t kSpinLimit = 1u << 22;
 
+// agg and incl are adjacent (one 16-byte load reads both); each is a
+// self-contained flag | value word.
 struct ChunkDesc {
   unsigned long long agg;       // kFlag | entries of the chunk
-  unsigned long long agg_nnz;
   unsigned long long incl;      // kFlag | entries of chunks 0..t
-  unsigned long long incl_nnz;
+  unsigned long long agg_nnz;   // (tiled kernel) nnz of the chunk, valid once agg is flagged
+  unsigned long long incl_nnz;  // (tiled kernel) nnz of chunks 0..t, valid once incl is flagged
 };
 
 struct FusedArgs {
@@ -68,6 +70,11 @@ struct FusedArgs {
   uint32_t nlevels;
   const uint64_t* lv_rowmap[kMaxLevels];
   const uint32_t* lv_entries[kMaxLevels];
+  // row mode: per CTA two staging buffers of stage_cap entries each, where a
+  // counted chunk's output waits while the chunk's prefix resolves; null:
+  // every chunk is written out in its own iteration
+  uint32_t* stage_buf;
+  uint32_t stage_cap;
 };
 
 // Row `row` of the (shifted) identity: column row + a_shift, or an empty

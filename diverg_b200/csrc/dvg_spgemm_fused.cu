@@ -608,6 +608,20 @@ static void* chunk_scratch(dvg_context* ctx, size_t desc_bytes) {
   return ctx->d_tile_desc;
 }
 
+// Staging for one single-pass row product on the context (null when the
+// deferred write-out is off).
+static uint32_t* stage_scratch(dvg_context* ctx, size_t bytes) {
+  if (!ctx->opt_row_stage || bytes == 0) return nullptr;
+  if (bytes > ctx->row_stage_cap) {
+    if (ctx->d_row_stage) dfree(ctx, ctx->d_row_stage);
+    ctx->d_row_stage = nullptr;
+    ctx->row_stage_cap = 0;
+    ctx->d_row_stage = static_cast<uint32_t*>(dalloc(ctx, bytes));
+    ctx->row_stage_cap = bytes;
+  }
+  return ctx->d_row_stage;
+}
+
 void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shift, uint64_t* c_rowmap,
                             uint32_t* c_entries, uint64_t cap) {
   if (u->nrows == 0) return;
@@ -630,6 +644,7 @@ void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shif
   L.desc = chunk_scratch(ctx, shape.desc_bytes);
   L.ticket = ctx->d_ticket;
   L.ctl = ctx->d_ctl;
+  L.stage_buf = stage_scratch(ctx, shape.stage_bytes);
   L.slot_variant = slot;
   launch_rowmode(ctx, L, shape);
 }
@@ -678,6 +693,7 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
     L.desc = chunk_scratch(ctx, shape.desc_bytes);
     L.ticket = ctx->d_ticket;
     L.ctl = ctx->d_ctl;
+    L.stage_buf = stage_scratch(ctx, shape.stage_bytes);
     L.slot_variant = slot;
     launch_rowmode(ctx, L, shape);
     return;

@@ -38,6 +38,7 @@ namespace {
 constexpr int kRowRowsMax = kChunkMax / kThreads;  // rows per thread at the largest chunk
 constexpr int kRowDirectWW = 192;  // warp path: 32-bit window words per warp (6,144 columns)
 constexpr int kAStage = 2048;      // A ranges of a chunk staged in shared memory
+constexpr int kRowStagePerRow = 16;  // staged entries per chunk row (a chunk with more is written in place)
 
 // The chunk's A row pointers and (up to kAStage of) its A ranges, loaded with
 // coalesced reads before the rows are walked; the warp path's windows reuse
@@ -51,18 +52,124 @@ union RowScratch {
   AStage a;
 };
 
+// Two chunks can be in flight per CTA: the one being counted (buffer b) and
+// the previous one (buffer b ^ 1), counted and staged in global memory,
+// waiting to be written out.
 template <int SLOT>
 struct RowSmem {
   uint32_t slot[SLOT * kThreads];       // entry k of thread t at [k * kThreads + t]
   RowScratch u;
-  uint32_t incl[kChunkMax];
-  uint32_t slow[kSlowMax];              // rows left to the warp-cooperative path
+  uint32_t incl[kChunkMax];             // the counted chunk's (then chunk-local inclusive) row counts
+  uint32_t slow[kSlowMax];              // rows of the counted chunk left to the warp path
   unsigned long long red[kWarps];
   unsigned long long red_nnz[kWarps];
-  unsigned long long prefix;
+  unsigned long long lb_sum[2][kWarps];  // look-back records by round parity, per warp
+  uint32_t lb_flag[2][kWarps];
+  uint32_t phase[kWarps];               // iterations per warp, checked at every iteration's end
+  unsigned long long pend_cnt;          // the staged chunk waiting in buffer b ^ 1
+  uint32_t pend_t, pend_crows;
   uint32_t next;                        // the chunk taken for the next iteration
   uint32_t nslow;
 };
+
+// CTA barrier that counts threads, not warps: the non-aligned form of
+// barrier.sync, which the lanes of a warp may reach at different times.  The
+// row loop leaves the lanes of a warp on paths of very different length (one
+// lane walks a wide row while the others wait), and the aligned form
+// (__syncthreads) is only defined for warps that arrive converged.  Every
+// barrier of the row kernel is this one, on barrier 0.
+__device__ __forceinline__ void cta_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
+
+// Publishes chunk t's aggregate (its entries) for later chunks' look-backs.
+__device__ __forceinline__ void publish_aggregate(const FusedArgs& p, uint32_t t, unsigned long long cnt) {
+  st_release(&p.desc[t].agg, kFlag | cnt);
+}
+
+// The whole CTA walks back from chunk t (whose aggregate is published),
+// kThreads descriptors a round, summing aggregates down to the nearest
+// inclusive prefix; every thread gets t's exclusive prefix and thread 0
+// publishes t's inclusive prefix (and, for the last chunk, the total).  A
+// deferred chunk's predecessors have mostly published aggregates but not yet
+// prefixes, so the walk is a few hundred descriptors deep: one round here.
+// A round is one 16-byte load per thread and one barrier: each warp reduces
+// its 32 descriptors (newest first) to a record -- the sum up to its first
+// prefix, whether it has one, whether a descriptor before that has nothing
+// yet -- and every thread scans the 16 records in order.  The records
+// alternate between two sets by round (`par` runs on across calls), so a
+// round's writes never meet the previous round's reads.  Waits are bounded;
+// every branch is uniform over the CTA.
+template <int SLOT>
+__device__ unsigned long long lookback_block(RowSmem<SLOT>& S, const FusedArgs& p, uint32_t t,
+                                             unsigned long long cnt, uint32_t& par) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  ChunkDesc* d = p.desc;
+  unsigned long long pre = 0;
+  int64_t j = int64_t(t) - 1;
+  uint32_t spins = 0;
+  while (j >= 0) {
+    const int64_t idx = j - tid;
+    int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: nothing yet
+    unsigned long long v = 0;
+    if (idx >= 0) {
+      unsigned long long va, vi;
+      asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(va), "=l"(vi) : "l"(&d[idx].agg) : "memory");
+      if (vi & kFlag) {
+        v = vi & ~kFlag;
+      } else if (va & kFlag) {
+        st = 1;
+        v = va & ~kFlag;
+      } else {
+        st = 0;
+      }
+    }
+    const unsigned im = __ballot_sync(kFullMask, st == 2), wm = __ballot_sync(kFullMask, st == 0);
+    const int fi = im ? __ffs(im) - 1 : 32;
+    const unsigned before = fi == 32 ? kFullMask : ((1u << fi) - 1u);
+    unsigned long long sv = lane <= fi ? v : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(kFullMask, sv, o);
+    if (lane == 0) {
+      S.lb_sum[par][warp] = sv;
+      S.lb_flag[par][warp] = (fi < 32 ? 1u : 0u) | ((wm & before) ? 2u : 0u);
+    }
+    cta_sync();
+    unsigned long long tot = 0;
+    bool done = false, wait = false;
+#pragma unroll 1
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t f = S.lb_flag[par][w];
+      if (f & 2u) {
+        wait = true;
+        break;
+      }
+      tot += S.lb_sum[par][w];
+      if (f & 1u) {
+        done = true;
+        break;
+      }
+    }
+    par ^= 1u;
+    if (wait) {  // a chunk after the nearest prefix has published nothing yet
+      if (++spins > kSpinLimit) {
+        if (tid == 0) raise_flag(p, &p.ctl->timeout, 1ull);
+        break;
+      }
+      __nanosleep(64);
+      continue;
+    }
+    pre += tot;
+    if (done) break;
+    j -= kThreads;
+  }
+  if (tid == 0) {
+    st_release(&d[t].incl, kFlag | (pre + cnt));
+    if (t == p.nchunks - 1) {
+      p.ctl->total = pre + cnt;
+      if (pre + cnt > p.cap) raise_flag(p, &p.ctl->overflow, pre + cnt);
+    }
+  }
+  return pre;
+}
 
 // Accumulates chunk row r (C row `row`) into the thread's slot from entry
 // `pos` on.  A's row pointers come from the stage, its ranges from the stage
@@ -199,6 +306,17 @@ __device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uin
 // The row kernel.  With rpt = ceil(chunk_rows / kThreads) rows per thread,
 // thread (warp, lane) owns chunk rows (warp * rpt + u) * 32 + lane, u < rpt:
 // the lanes of a warp take consecutive rows.
+//
+// An iteration counts chunk t into buffer b: stage A, walk the rows into the
+// slots, count the rows that missed the slots on the warp path, the
+// chunk-local prefix.  When the CTA has a staging area (p.stage_buf) and the
+// chunk's runs fit it, the iteration publishes t's aggregate and writes the
+// chunk's complete image -- every row's runs at its chunk-local offset -- to
+// staging buffer b, and resolves t one iteration later: by then the chunks
+// before it have long published their aggregates, so the look-back rarely
+// waits, and the write-out is the row map plus one coalesced copy.  Any
+// other chunk is resolved in its own iteration (look-back, then rows written
+// in place).  Every barrier of the loop is reached by the whole CTA.
 template <bool A_ID, int SLOT>
 __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -207,6 +325,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   uint32_t* dbits = S.u.direct + size_t(warp) * 2 * kRowDirectWW;
   uint32_t* dreach = dbits + kRowDirectWW;
   const uint32_t rpt = (p.chunk_rows + kThreads - 1) / kThreads;  // 1..kRowRowsMax
+  // per CTA two buffers: a chunk's image (stage_cap entries), then its
+  // chunk-local inclusive row counts (chunk_rows words)
+  uint32_t* const stage =
+      p.stage_buf ? p.stage_buf + size_t(blockIdx.x) * 2 * (p.stage_cap + p.chunk_rows) : nullptr;
   // a planned build stops at the first step whose output is unusable
   auto take_ticket = [&]() -> uint32_t {
     const bool stop = p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
@@ -216,172 +338,289 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     S.next = take_ticket();
     S.nslow = 0;
   }
-  __syncthreads();
-  uint32_t t = S.next;
-  while (t < p.nchunks) {
-    const uint32_t c0row = t * p.chunk_rows;
-    const uint32_t crows = min(p.chunk_rows, p.nrows - c0row);
-    // stage A's row pointers and ranges of the chunk (coalesced)
-    uint64_t abase = 0;
-    uint32_t nst = 0;
-    if (!A_ID) {
-      for (uint32_t r = tid; r <= crows; r += kThreads) S.u.a.arow[r] = __ldg(p.a_rowmap + uint64_t(c0row) + r);
-      __syncthreads();
-      abase = S.u.a.arow[0] >> 1;
-      const uint64_t nrange = (S.u.a.arow[crows] >> 1) - abase;
-      nst = nrange < uint64_t(kAStage) ? uint32_t(nrange) : uint32_t(kAStage);
-      for (uint32_t k = tid; k < nst; k += kThreads) S.u.a.aent[k] = load_range(p.a_entries, abase + k);
-      __syncthreads();
-    }
-    unsigned long long nnz_acc = 0;
-    uint32_t fast_mask = 0, pos = 0;
-    // rows that miss the slot wait for the warp-cooperative pass below, so
-    // one wide row never holds a whole chunk behind a single thread
-#pragma unroll
-    for (int u = 0; u < kRowRowsMax; ++u) {
-      if (uint32_t(u) >= rpt) break;
-      const uint32_t r = (warp * rpt + u) * 32 + lane;
-      if (r < crows) {
-        uint32_t cnt = 0;
-        if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, r, abase, nst, pos, cnt, nnz_acc)) {
-          fast_mask |= 1u << u;
-          pos += cnt;
-        } else {
-          const uint32_t i = atomicAdd(&S.nslow, 1u);
-          if (i < uint32_t(kSlowMax)) {
-            S.slow[i] = r;
-          } else {
-            cnt = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
-          }
-          atomicAdd(&p.ctl->slow_rows, 1ull);
-        }
-        S.incl[r] = cnt;
+  cta_sync();
+  uint32_t t = S.next, b = 0, par = 0;
+  bool pend = false;  // a staged chunk waits in buffer b ^ 1 (described in S.pend_*)
+  uint32_t iter = 0;
+  while (t < p.nchunks || pend) {
+    const bool have = t < p.nchunks;
+    // thread 0 takes the next ticket while the rows are walked (its latency
+    // hides behind the chunk); a planned build takes none once aborted
+    const bool stop = tid == 0 && p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
+    uint32_t next = 0xffffffffu;
+    const uint32_t c0row = have ? t * p.chunk_rows : 0u;
+    const uint32_t crows = have ? min(p.chunk_rows, p.nrows - c0row) : 0u;
+    uint32_t* const incl = S.incl;
+    unsigned long long nnz_acc = 0, cnt = 0, cnnz = 0;
+    uint32_t fast_mask = 0, nslow = 0, nslow_all = 0;
+    bool staged = false;
+    if (have) {
+      // stage A's row pointers and ranges of the chunk (coalesced)
+      uint64_t abase = 0;
+      uint32_t nst = 0;
+      if (!A_ID) {
+        for (uint32_t r = tid; r <= crows; r += kThreads) S.u.a.arow[r] = __ldg(p.a_rowmap + uint64_t(c0row) + r);
+        cta_sync();
+        abase = S.u.a.arow[0] >> 1;
+        const uint64_t nrange = (S.u.a.arow[crows] >> 1) - abase;
+        nst = nrange < uint64_t(kAStage) ? uint32_t(nrange) : uint32_t(kAStage);
+        for (uint32_t k = tid; k < nst; k += kThreads) S.u.a.aent[k] = load_range(p.a_entries, abase + k);
+        cta_sync();
       }
-    }
-    __syncthreads();
-    // the stage is dead from here on: the warp path may use the space
-    const uint32_t nslow_all = S.nslow;
-    const uint32_t nslow = min(nslow_all, uint32_t(kSlowMax));
-    if (nslow) {
-      for (uint32_t i = warp; i < nslow; i += kWarps) {
-        const uint32_t r = S.slow[i];
-        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
-                                      [](uint64_t, uint32_t) {}, kRowDirectWW);
-        if (lane == 0) S.incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
-      }
-      __syncthreads();
-    }
-    // chunk prefix over the row counts (kRowRowsMax consecutive rows per
-    // thread: a thread rewrites only its own rows) and the chunk's nnz
-    {
-      uint32_t loc[kRowRowsMax];
-      uint64_t s = 0;
-#pragma unroll
-      for (int k = 0; k < kRowRowsMax; ++k) {
-        const uint32_t r = tid * kRowRowsMax + k;
-        s += r < crows ? S.incl[r] : 0u;
-        loc[k] = uint32_t(s);
-      }
-      uint64_t inc = s;
-      unsigned long long v = nnz_acc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint64_t u = __shfl_up_sync(kFullMask, inc, o);
-        if (lane >= o) inc += u;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
-      if (lane == 31) S.red[warp] = inc;
-      if (lane == 0) S.red_nnz[warp] = v;
-      __syncthreads();
-      uint64_t wpre = 0;
-      for (int i = 0; i < warp; ++i) wpre += S.red[i];
-      const uint64_t excl = wpre + inc - s;
-      if (excl + s > 0xffffffffull) raise_flag(p, &p.ctl->status, 16ull);
-#pragma unroll
-      for (int k = 0; k < kRowRowsMax; ++k) {
-        const uint32_t r = tid * kRowRowsMax + k;
-        if (r < crows) S.incl[r] = uint32_t(excl) + loc[k];
-      }
-    }
-    __syncthreads();
-    if (warp == 0) {
-      unsigned long long chunk_nnz = 0;
-      for (int i = 0; i < kWarps; ++i) chunk_nnz += S.red_nnz[i];
-      const unsigned long long chunk_cnt = S.incl[crows - 1];
-      unsigned long long pre, pre_nnz;
-      lookback_warp(p, t, chunk_cnt, chunk_nnz, pre, pre_nnz);
-      if (lane == 0) {
-        S.prefix = pre;
-        if (t == p.nchunks - 1) {
-          p.ctl->total = pre + chunk_cnt;
-          p.ctl->nnz = pre_nnz + chunk_nnz;
-          if (pre + chunk_cnt > p.cap) raise_flag(p, &p.ctl->overflow, pre + chunk_cnt);
-        }
-      }
-    }
-    __syncthreads();
-    // the next chunk is taken now; its counts start from zero
-    if (tid == 0) {
-      S.next = take_ticket();
-      S.nslow = 0;
-    }
-    const unsigned long long prefix = S.prefix;
-    for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + S.incl[r];
-    if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
-    pos = 0;
-#pragma unroll
-    for (int u = 0; u < kRowRowsMax; ++u) {
-      if (uint32_t(u) >= rpt) break;
-      const uint32_t r = (warp * rpt + u) * 32 + lane;
-      if (r >= crows) continue;
-      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
-      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
-      const bool fast = (fast_mask >> u) & 1u;
-      if (n && dst + n > p.cap) {
-        raise_flag(p, &p.ctl->overflow, 1ull);
-      } else if (fast) {
-        for (uint32_t k = 0; k < n; ++k) p.c_entries[dst + k] = S.slot[(pos + k) * kThreads + tid];
-      }
-      if (fast) pos += n;
-    }
-    // rows that missed the slot: the listed ones by warps, any overflow of
-    // the list by its own thread
-    for (uint32_t i = warp; i < nslow; i += kWarps) {
-      const uint32_t r = S.slow[i];
-      const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
-      const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
-      if (n == 0 || dst + n > p.cap) continue;
-      uint32_t* out = p.c_entries + dst;
-      bool bad = false;
-      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
-                                    [&](uint64_t k, uint32_t v) {
-                                      if (k < n) out[k] = v;
-                                      else bad = true;
-                                    },
-                                    kRowDirectWW);
-      if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
-    }
-    if (nslow_all > uint32_t(kSlowMax)) {
+      uint32_t pos = 0;
+      // rows that miss the slot wait for the warp-cooperative pass below, so
+      // one wide row never holds a whole chunk behind a single thread
 #pragma unroll
       for (int u = 0; u < kRowRowsMax; ++u) {
         if (uint32_t(u) >= rpt) break;
         const uint32_t r = (warp * rpt + u) * 32 + lane;
-        if (r >= crows || ((fast_mask >> u) & 1u)) continue;
-        bool listed = false;
-        for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
-        if (listed) continue;
-        const unsigned long long dst = prefix + (r ? S.incl[r - 1] : 0u);
-        const uint32_t n = S.incl[r] - (r ? S.incl[r - 1] : 0u);
-        if (n == 0 || dst + n > p.cap) continue;
-        uint32_t* out = p.c_entries + dst;
-        uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr, [&](uint64_t k, uint32_t v) {
-          if (k < n) out[k] = v;
-        });
-        if (c != n) raise_flag(p, &p.ctl->status, 8ull);
+        if (r < crows) {
+          uint32_t c = 0;
+          if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, r, abase, nst, pos, c, nnz_acc)) {
+            fast_mask |= 1u << u;
+            pos += c;
+          } else {
+            const uint32_t i = atomicAdd(&S.nslow, 1u);
+            if (i < uint32_t(kSlowMax)) {
+              S.slow[i] = r;
+            } else {
+              c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
+            }
+            atomicAdd(&p.ctl->slow_rows, 1ull);
+          }
+          incl[r] = c;
+        }
+      }
+      cta_sync();
+      if (tid == 0 && !stop) next = atomicAdd(p.ticket, 1u);
+      // the stage is dead from here on: the warp path may use the space
+      nslow_all = S.nslow;
+      nslow = min(nslow_all, uint32_t(kSlowMax));
+      for (uint32_t i = warp; i < nslow; i += kWarps) {
+        const uint32_t r = S.slow[i];
+        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
+                                      [](uint64_t, uint32_t) {}, kRowDirectWW);
+        if (lane == 0) incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+      }
+      cta_sync();
+      // chunk prefix over the row counts (kRowRowsMax consecutive rows per
+      // thread: a thread rewrites only its own rows) and the chunk's nnz
+      {
+        uint32_t loc[kRowRowsMax];
+        uint64_t s = 0;
+#pragma unroll
+        for (int k = 0; k < kRowRowsMax; ++k) {
+          const uint32_t r = tid * kRowRowsMax + k;
+          s += r < crows ? incl[r] : 0u;
+          loc[k] = uint32_t(s);
+        }
+        uint64_t inc = s;
+        unsigned long long v = nnz_acc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          uint64_t u = __shfl_up_sync(kFullMask, inc, o);
+          if (lane >= o) inc += u;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+        if (lane == 31) S.red[warp] = inc;
+        if (lane == 0) S.red_nnz[warp] = v;
+        cta_sync();
+        uint64_t wpre = 0;
+        for (int i = 0; i < warp; ++i) wpre += S.red[i];
+        const uint64_t excl = wpre + inc - s;
+        if (excl + s > 0xffffffffull) raise_flag(p, &p.ctl->status, 16ull);
+#pragma unroll
+        for (int k = 0; k < kRowRowsMax; ++k) {
+          const uint32_t r = tid * kRowRowsMax + k;
+          if (r < crows) incl[r] = uint32_t(excl) + loc[k];
+        }
+      }
+      cta_sync();
+      for (int i = 0; i < kWarps; ++i) cnnz += S.red_nnz[i];
+      cnt = incl[crows - 1];
+      if (tid == 0) atomicAdd(&p.ctl->nnz, cnnz);
+      staged = stage != nullptr && cnt <= p.stage_cap;
+      if (staged) {
+        // the chunk's image: fast rows from the slots, the rest recomputed
+        uint32_t* img = stage + size_t(b) * (p.stage_cap + p.chunk_rows);
+        if (tid == 0) publish_aggregate(p, t, cnt);
+        for (uint32_t r = tid; r < crows; r += kThreads) img[p.stage_cap + r] = incl[r];
+        uint32_t spos = 0;
+#pragma unroll
+        for (int u = 0; u < kRowRowsMax; ++u) {
+          if (uint32_t(u) >= rpt) break;
+          const uint32_t r = (warp * rpt + u) * 32 + lane;
+          if (r >= crows || !((fast_mask >> u) & 1u)) continue;
+          const uint32_t o = r ? incl[r - 1] : 0u;
+          const uint32_t n = incl[r] - o;
+          for (uint32_t k = 0; k < n; ++k) img[o + k] = S.slot[(spos + k) * kThreads + tid];
+          spos += n;
+        }
+        for (uint32_t i = warp; i < nslow; i += kWarps) {
+          const uint32_t r = S.slow[i];
+          const uint32_t o = r ? incl[r - 1] : 0u;
+          const uint32_t n = incl[r] - o;
+          if (n == 0) continue;
+          bool bad = false;
+          const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
+                                        [&](uint64_t k, uint32_t v) {
+                                          if (k < n) img[o + k] = v;
+                                          else bad = true;
+                                        },
+                                        kRowDirectWW);
+          if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+        }
+        if (nslow_all > uint32_t(kSlowMax)) {
+#pragma unroll
+          for (int u = 0; u < kRowRowsMax; ++u) {
+            if (uint32_t(u) >= rpt) break;
+            const uint32_t r = (warp * rpt + u) * 32 + lane;
+            if (r >= crows || ((fast_mask >> u) & 1u)) continue;
+            bool listed = false;
+            for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
+            if (listed) continue;
+            const uint32_t o = r ? incl[r - 1] : 0u;
+            const uint32_t n = incl[r] - o;
+            if (n == 0) continue;
+            const uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
+                                               [&](uint64_t k, uint32_t v) {
+                                                 if (k < n) img[o + k] = v;
+                                               });
+            if (c != n) raise_flag(p, &p.ctl->status, 8ull);
+          }
+        }
       }
     }
-    __syncthreads();
+    // every thread is done with the slots, the slow list and the counted
+    // chunk's image; the warp path's windows are free again
+    cta_sync();
+    // the pending chunk: look-back, row map, one coalesced copy
+    if (pend) {
+      const uint32_t pend_t = S.pend_t, pend_crows = S.pend_crows;
+      const unsigned long long pend_cnt = S.pend_cnt;
+      const unsigned long long prefix = lookback_block(S, p, pend_t, pend_cnt, par);
+      const uint32_t* img = stage + size_t(b ^ 1u) * (p.stage_cap + p.chunk_rows);
+      const uint32_t* pincl = img + p.stage_cap;
+      const uint32_t p0row = pend_t * p.chunk_rows;
+      // loads first, then stores: the staging and the output may alias as
+      // far as the compiler knows, and a load after a store would wait
+      {
+        uint32_t v[kRowRowsMax];
+#pragma unroll
+        for (int u = 0; u < kRowRowsMax; ++u) {
+          const uint32_t r = tid + u * kThreads;
+          v[u] = r < pend_crows ? __ldcg(pincl + r) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kRowRowsMax; ++u) {
+          const uint32_t r = tid + u * kThreads;
+          if (r < pend_crows) p.c_rowmap[uint64_t(p0row) + r + 1] = prefix + v[u];
+        }
+      }
+      if (pend_t == 0 && tid == 0) p.c_rowmap[0] = 0;
+      if (prefix + pend_cnt <= p.cap) {
+        uint32_t* dst = p.c_entries + prefix;
+        constexpr int kBatch = 8;
+        for (uint64_t k0 = 0; k0 < pend_cnt; k0 += uint64_t(kBatch) * kThreads) {
+          uint32_t v[kBatch];
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u) {
+            const uint64_t k = k0 + tid + uint64_t(u) * kThreads;
+            v[u] = k < pend_cnt ? __ldcg(img + k) : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u) {
+            const uint64_t k = k0 + tid + uint64_t(u) * kThreads;
+            if (k < pend_cnt) dst[k] = v[u];
+          }
+        }
+      } else if (tid == 0 && pend_cnt) {
+        raise_flag(p, &p.ctl->overflow, 1ull);
+      }
+      pend = false;
+    }
+    // a counted chunk that was not staged is resolved now, in place
+    if (have && !staged) {
+      if (tid == 0) publish_aggregate(p, t, cnt);
+      const unsigned long long prefix = lookback_block(S, p, t, cnt, par);
+      for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + incl[r];
+      if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
+      uint32_t pos = 0;
+#pragma unroll
+      for (int u = 0; u < kRowRowsMax; ++u) {
+        if (uint32_t(u) >= rpt) break;
+        const uint32_t r = (warp * rpt + u) * 32 + lane;
+        if (r >= crows) continue;
+        const unsigned long long dst = prefix + (r ? incl[r - 1] : 0u);
+        const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
+        const bool fast = (fast_mask >> u) & 1u;
+        if (n && dst + n > p.cap) {
+          raise_flag(p, &p.ctl->overflow, 1ull);
+        } else if (fast) {
+          for (uint32_t k = 0; k < n; ++k) p.c_entries[dst + k] = S.slot[(pos + k) * kThreads + tid];
+        }
+        if (fast) pos += n;
+      }
+      for (uint32_t i = warp; i < nslow; i += kWarps) {
+        const uint32_t r = S.slow[i];
+        const unsigned long long dst = prefix + (r ? incl[r - 1] : 0u);
+        const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
+        if (n == 0 || dst + n > p.cap) continue;
+        uint32_t* out = p.c_entries + dst;
+        bool bad = false;
+        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
+                                      [&](uint64_t k, uint32_t v) {
+                                        if (k < n) out[k] = v;
+                                        else bad = true;
+                                      },
+                                      kRowDirectWW);
+        if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+      }
+      if (nslow_all > uint32_t(kSlowMax)) {
+#pragma unroll
+        for (int u = 0; u < kRowRowsMax; ++u) {
+          if (uint32_t(u) >= rpt) break;
+          const uint32_t r = (warp * rpt + u) * 32 + lane;
+          if (r >= crows || ((fast_mask >> u) & 1u)) continue;
+          bool listed = false;
+          for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
+          if (listed) continue;
+          const unsigned long long dst = prefix + (r ? incl[r - 1] : 0u);
+          const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
+          if (n == 0 || dst + n > p.cap) continue;
+          uint32_t* out = p.c_entries + dst;
+          uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
+                                       [&](uint64_t k, uint32_t v) {
+                                         if (k < n) out[k] = v;
+                                       });
+          if (c != n) raise_flag(p, &p.ctl->status, 8ull);
+        }
+      }
+    }
+    if (staged) {
+      pend = true;
+      b ^= 1u;
+    }
+    // the next chunk; every warp must have passed the same barriers
+    ++iter;
+    if (lane == 0) S.phase[warp] = iter;
+    if (tid == 0) {
+      if (staged) {
+        S.pend_t = t;
+        S.pend_crows = crows;
+        S.pend_cnt = cnt;
+      }
+      S.next = next;
+      S.nslow = 0;
+    }
+    cta_sync();
+    if (tid == 0) {
+      bool same = true;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) same = same && S.phase[w] == iter;
+      if (!same) raise_flag(p, &p.ctl->status, 64ull);
+    }
     t = S.next;
   }
 }
@@ -424,6 +663,7 @@ RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_
   s.nchunks = uint32_t((uint64_t(nrows) + chunk_rows - 1) / chunk_rows);
   s.grid = uint32_t(std::min<uint64_t>(s.nchunks, s.resident));
   s.desc_bytes = size_t(s.nchunks) * sizeof(ChunkDesc);
+  s.stage_bytes = size_t(s.grid) * 2 * (kRowStagePerRow + 1) * s.chunk_rows * sizeof(uint32_t);
   return s;
 }
 
@@ -449,6 +689,8 @@ void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& 
   p.d_entries = L.d_identity ? nullptr : L.d_entries;
   p.d_identity = L.d_identity ? 1u : 0u;
   p.abort = L.abort;
+  p.stage_buf = L.stage_buf;
+  p.stage_cap = L.stage_buf ? uint32_t(kRowStagePerRow) * s.chunk_rows : 0u;
   p.a_shift = L.a_identity ? L.a_shift : 0u;
   p.b_nrows = L.b_nrows;
   p.nlevels = L.nlevels;

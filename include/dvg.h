@@ -104,7 +104,11 @@ dvg_status dvg_synchronize(dvg_context* ctx);
  * capacity of every step as a percentage of the input's entries, 300 by
  * default and adapted after each build; a step that outgrows it makes the
  * build re-run on the read-back path), "row_slot" (thread-per-row kernel: run-list
- * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "spgemm_levels"
+ * entries per thread, 0 = 16, 1 = 24, the default, 2 = 32), "row_stage"
+ * (thread-per-row kernel: 1 = a counted chunk's output waits in a staging
+ * buffer, 16 entries a row for two chunks per CTA, while its offset resolves,
+ * and is copied out one iteration later, the default; 0 = every chunk waits
+ * for its offset and is written out in its own iteration), "spgemm_levels"
  * (1 = a thread-per-row product whose A ranges average 4 or more rows -- up
  * to 8 in automatic mode, which stages tiles above that -- first builds union
  * levels of B -- level k row j is the union of B's rows j .. j + 2^k - 1 --
