@@ -80,6 +80,15 @@ struct RowSmem {
 // barrier of the row kernel is this one, on barrier 0.
 __device__ __forceinline__ void cta_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
 
+// Asynchronous 8-byte copy global -> shared (cp.async): the copy lands while
+// the thread goes on; cp_async_wait() waits for all of the thread's copies.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const uint32_t sa = uint32_t(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Publishes chunk t's aggregate (its entries) for later chunks' look-backs.
 __device__ __forceinline__ void publish_aggregate(const FusedArgs& p, uint32_t t, unsigned long long cnt) {
   st_release(&p.desc[t].agg, kFlag | cnt);
@@ -341,6 +350,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   cta_sync();
   uint32_t t = S.next, b = 0, par = 0;
   bool pend = false;  // a staged chunk waits in buffer b ^ 1 (described in S.pend_*)
+  bool pre = false;   // the A stage of chunk t was requested during the previous iteration
+  // the asynchronous stage copies 8-byte words
+  const bool a_async = !A_ID && ((reinterpret_cast<uintptr_t>(p.a_rowmap) | reinterpret_cast<uintptr_t>(p.a_entries)) & 7u) == 0;
   uint32_t iter = 0;
   while (t < p.nchunks || pend) {
     const bool have = t < p.nchunks;
@@ -359,13 +371,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       uint64_t abase = 0;
       uint32_t nst = 0;
       if (!A_ID) {
-        for (uint32_t r = tid; r <= crows; r += kThreads) S.u.a.arow[r] = __ldg(p.a_rowmap + uint64_t(c0row) + r);
-        cta_sync();
+        if (pre) {
+          // requested during the previous iteration
+          cp_async_wait();
+          cta_sync();
+        } else {
+          for (uint32_t r = tid; r <= crows; r += kThreads) S.u.a.arow[r] = __ldg(p.a_rowmap + uint64_t(c0row) + r);
+          cta_sync();
+        }
         abase = S.u.a.arow[0] >> 1;
         const uint64_t nrange = (S.u.a.arow[crows] >> 1) - abase;
         nst = nrange < uint64_t(kAStage) ? uint32_t(nrange) : uint32_t(kAStage);
-        for (uint32_t k = tid; k < nst; k += kThreads) S.u.a.aent[k] = load_range(p.a_entries, abase + k);
-        cta_sync();
+        if (!pre) {
+          for (uint32_t k = tid; k < nst; k += kThreads) S.u.a.aent[k] = load_range(p.a_entries, abase + k);
+          cta_sync();
+        }
       }
       uint32_t pos = 0;
       // rows that miss the slot wait for the warp-cooperative pass below, so
@@ -492,9 +512,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         }
       }
     }
+    if (tid == 0) S.next = next;
     // every thread is done with the slots, the slow list and the counted
     // chunk's image; the warp path's windows are free again
     cta_sync();
+    // after a staged chunk the shared stage stays free until the next
+    // iteration: request the next chunk's A row pointers now, its ranges once
+    // those have landed, so both arrive behind the pending chunk's write-out
+    pre = !A_ID && have && staged && S.next < p.nchunks && a_async;
+    uint32_t n0row = 0, nrows1 = 0;
+    if (pre) {
+      n0row = S.next * p.chunk_rows;
+      nrows1 = min(p.chunk_rows, p.nrows - n0row);
+      for (uint32_t r = tid; r <= nrows1; r += kThreads) cp_async8(&S.u.a.arow[r], p.a_rowmap + uint64_t(n0row) + r);
+      cp_async_commit();
+    }
     // the pending chunk: look-back, row map, one coalesced copy
     if (pend) {
       const uint32_t pend_t = S.pend_t, pend_crows = S.pend_crows;
@@ -539,6 +571,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         raise_flag(p, &p.ctl->overflow, 1ull);
       }
       pend = false;
+    }
+    if (pre) {
+      cp_async_wait();
+      cta_sync();
+      const uint64_t nbase = S.u.a.arow[0] >> 1;
+      const uint64_t nrange = (S.u.a.arow[nrows1] >> 1) - nbase;
+      const uint32_t nst1 = nrange < uint64_t(kAStage) ? uint32_t(nrange) : uint32_t(kAStage);
+      for (uint32_t k = tid; k < nst1; k += kThreads) cp_async8(&S.u.a.aent[k], p.a_entries + 2 * (nbase + k));
+      cp_async_commit();
     }
     // a counted chunk that was not staged is resolved now, in place
     if (have && !staged) {
@@ -611,7 +652,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         S.pend_crows = crows;
         S.pend_cnt = cnt;
       }
-      S.next = next;
       S.nslow = 0;
     }
     cta_sync();
