@@ -39,8 +39,8 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per C row of the row kernel, mean of the four
 # launches of profiles/k_spgemm_rowmode_index_1e7.md (ncu, 10,019,292-row
 # graph): traffic scales with the rows of the product
-ROWMODE_TRAFFIC_BYTES_PER_ROW = (482445568 + 322691584 + 325835776 + 326179072 +
-                                 136677376 + 129849600 + 134458880 + 128670720) / 4 / 10019292
+ROWMODE_TRAFFIC_BYTES_PER_ROW = (485766656 + 323889664 + 329825792 + 327297024 +
+                                 154642944 + 139796480 + 150942464 + 137347328) / 4 / 10019292
 
 
 def parse_args():
@@ -402,14 +402,18 @@ def main():
         barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
+        wall = []
         for _ in range(args.steps):
+            w0 = time.perf_counter()
             idx = ctx.distance_index(d_a, args.dmin, args.dmax)
             idx.free()
+            wall.append((time.perf_counter() - w0) * 1e3)
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
     ms_total = max_over_ranks(ev0.elapsed_time(ev1))
-    launches = ctx.stats()["kernel_launches"]
+    st_timed = ctx.stats()
+    launches = st_timed["kernel_launches"]
     sec_per_build = ms_total / 1e3 / args.steps
 
     # ---- the same builds again with per-kernel event spans (roofline) ------
@@ -488,6 +492,13 @@ def main():
                           "spgemm_numeric": st["spgemm_numeric_ns"] / 1e6 / steps,
                           "scan": st["scan_ns"] / 1e6 / steps, "spadd": st["spadd_ns"] / 1e6 / steps},
                       "host_syncs_per_build": st["host_syncs"] / steps,
+                      # host side of the timed builds: where the GPU could idle
+                      "host_ms_per_build": {
+                          "wall_per_step": [round(w, 2) for w in wall],
+                          "prepare": st_timed["host_prepare_ns"] / 1e6 / steps,
+                          "meminfo": st_timed["host_meminfo_ns"] / 1e6 / steps,
+                          "launch": st_timed["host_launch_ns"] / 1e6 / steps,
+                          "sync_wait": st_timed["host_sync_ns"] / 1e6 / steps},
                       "range_ops_per_build": st["range_ops"] / steps},
         }
         print(json.dumps(line), flush=True)
