@@ -69,7 +69,8 @@ class Completion(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "builds_submitted", "builds_done", "build_batches", "queries_submitted", "queries_done", "pairs_answered",
-        "resident_bytes", "peak_reserved_bytes", "hbm_budget_bytes")]
+        "resident_bytes", "peak_reserved_bytes", "hbm_budget_bytes", "build_reruns", "build_batch_ns_max",
+        "build_alloc_ns", "build_sync_ns")]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

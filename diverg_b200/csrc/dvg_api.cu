@@ -67,6 +67,7 @@ uint64_t now_ns() {
 static void release_cached(dvg_context* ctx) {
   for (auto& kv : ctx->free_blocks) DVG_CUDA(cudaFreeAsync(kv.second, ctx->stream));
   ctx->free_blocks.clear();
+  ctx->owned_bytes -= std::min(ctx->owned_bytes, ctx->cached_bytes);
   ctx->cached_bytes = 0;
 }
 
@@ -75,9 +76,21 @@ static void release_cached(dvg_context* ctx) {
 // goes to cudaMallocAsync, and when that fails the cache is released and the
 // request retried once.  Re-mapping GB-sized buffers in the pool on every
 // product costs tens to hundreds of milliseconds per index build.
+// Allocation sizes are rounded up to classes -- 256-byte granules up to
+// 1 MiB, above that quarter steps of a power of two (at most 25 % more) -- so
+// the requests of differently sized builds meet in the cache instead of each
+// growing the pool.
+static size_t size_class(size_t bytes) {
+  bytes = (std::max<size_t>(bytes, 16) + 255) & ~size_t(255);
+  if (bytes <= (size_t(1) << 20)) return bytes;
+  const int k = 63 - __builtin_clzll(uint64_t(bytes));
+  const size_t step = size_t(1) << (k - 2);
+  return (bytes + step - 1) & ~(step - 1);
+}
+
 void* dalloc(dvg_context* ctx, size_t bytes) {
   const uint64_t t0 = now_ns();
-  bytes = (std::max<size_t>(bytes, 16) + 255) & ~size_t(255);
+  bytes = size_class(bytes);
   auto it = ctx->free_blocks.lower_bound(bytes);
   if (it != ctx->free_blocks.end() && it->first <= bytes + bytes / 4) {
     void* p = it->second;
@@ -102,7 +115,30 @@ void* dalloc(dvg_context* ctx, size_t bytes) {
                 std::string("device allocation of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
   }
   ctx->live_blocks[p] = bytes;
+  ctx->owned_bytes += bytes;
   return p;
+}
+
+// Free device memory for planning.  cudaMemGetInfo is a driver round trip
+// that has taken tens of milliseconds on a busy machine, so an answer is
+// reused for up to a second, corrected by what this context has allocated
+// or released since.  A plan sized on a stale answer fails its allocation
+// and falls back like any other out-of-memory plan.
+size_t device_free_bytes(dvg_context* ctx) {
+  constexpr uint64_t kTtlNs = 1000000000ull;
+  const uint64_t t0 = now_ns();
+  if (ctx->mi_ns == 0 || t0 - ctx->mi_ns > kTtlNs) {
+    size_t free_b = 0, total_b = 0;
+    DVG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    ctx->mi_ns = now_ns();
+    ctx->stats.host_meminfo_ns += ctx->mi_ns - t0;
+    ctx->mi_free = free_b;
+    ctx->mi_owned = ctx->owned_bytes;
+    return free_b;
+  }
+  const size_t grew = ctx->owned_bytes > ctx->mi_owned ? ctx->owned_bytes - ctx->mi_owned : 0;
+  const size_t shrank = ctx->mi_owned > ctx->owned_bytes ? ctx->mi_owned - ctx->owned_bytes : 0;
+  return grew >= ctx->mi_free + shrank ? 0 : ctx->mi_free + shrank - grew;
 }
 
 void dfree(dvg_context* ctx, void* p) {
@@ -698,6 +734,8 @@ dvg_status dvg_shutdown(dvg_context* ctx) {
     DVG_CUDA(cudaFree(ctx->d_ctl));
     DVG_CUDA(cudaFreeHost(ctx->h_ctl));
     if (ctx->h_stage) DVG_CUDA(cudaFreeHost(ctx->h_stage));
+    for (void* h : ctx->h_retired) DVG_CUDA(cudaFreeHost(h));
+    ctx->h_retired.clear();
     if (ctx->own_stream) DVG_CUDA(cudaStreamDestroy(ctx->own_stream));
   });
   delete ctx;

@@ -25,13 +25,16 @@
 
 namespace dvg {
 
+// Pinned host staging for read-backs.  It grows by doubling, and a buffer it
+// outgrows is kept until the context shuts down: cudaFreeHost waits for the
+// whole device, which would stall every other stream (a server's queries).
 void* host_stage(dvg_context* ctx, size_t bytes) {
   if (bytes > ctx->h_stage_cap) {
-    if (ctx->h_stage) DVG_CUDA(cudaFreeHost(ctx->h_stage));
-    ctx->h_stage = nullptr;
-    ctx->h_stage_cap = 0;
-    const size_t want = std::max<size_t>(bytes, 64 << 10);
-    DVG_CUDA(cudaMallocHost(&ctx->h_stage, want));
+    const size_t want = std::max<size_t>({bytes, 2 * ctx->h_stage_cap, size_t(64) << 10});
+    void* p = nullptr;
+    DVG_CUDA(cudaMallocHost(&p, want));
+    if (ctx->h_stage) ctx->h_retired.push_back(ctx->h_stage);
+    ctx->h_stage = p;
     ctx->h_stage_cap = want;
   }
   return ctx->h_stage;
@@ -136,10 +139,7 @@ PlannedBuild prepare_build(dvg_context* ctx, const IndexPlan& plan, const dvg_ma
   uint64_t est = std::max<uint64_t>(uint64_t(ctx->plan_growth * double(a->nentries)), 4ull * pb.n) + 64;
   // keep the plan within 80 % of the memory the device (and this context's
   // cache) can give; a step that then overflows re-runs on the read-back path
-  size_t free_b = 0, total_b = 0;
-  const uint64_t tm = now_ns();
-  DVG_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  ctx->stats.host_meminfo_ns += now_ns() - tm;
+  const size_t free_b = device_free_bytes(ctx);
   const double avail = 0.8 * double(free_b + ctx->cached_bytes) / double(max_live) - 8.0 * (double(pb.n) + 1);
   if (avail < 4.0 * double(est)) est = std::max<uint64_t>(uint64_t(std::max(avail, 0.0) / 4.0), 4ull * pb.n + 64);
   try {

@@ -82,6 +82,7 @@ struct dvg_context {
   std::map<std::tuple<unsigned, unsigned, int>, TuneChoice> tuned;
   void* h_stage = nullptr;            // pinned host staging for read-backs
   size_t h_stage_cap = 0;
+  std::vector<void*> h_retired;       // outgrown pinned buffers, freed at shutdown
   bool opt_timing = false;
   // event pairs bracketing timed kernels, resolved at the next stream sync
   struct TimedSpan {
@@ -95,6 +96,10 @@ struct dvg_context {
   std::multimap<size_t, void*> free_blocks;      // bytes -> block
   std::unordered_map<void*, size_t> live_blocks;  // block -> bytes
   size_t cached_bytes = 0;
+  size_t owned_bytes = 0;   // device memory this context holds (live + cached)
+  // the last cudaMemGetInfo answer, when it was taken, and owned_bytes then
+  size_t mi_free = 0, mi_owned = 0;
+  uint64_t mi_ns = 0;
 };
 
 namespace dvg {
@@ -114,6 +119,7 @@ void record_error(const std::string& msg);
 
 void* dalloc(dvg_context* ctx, size_t bytes);
 void dfree(dvg_context* ctx, void* p);
+size_t device_free_bytes(dvg_context* ctx);  // free device memory for planning (cached query)
 
 // A device matrix owned by the context's allocator.
 dvg_matrix* new_matrix(dvg_context* ctx, uint32_t nrows, uint32_t ncols, uint64_t nentries);

@@ -73,7 +73,8 @@ struct QuerySlot {
   uint32_t* h_pairs = nullptr;
   uint8_t* h_out = nullptr;
   DeviceControl* h_ctl = nullptr;
-  uint64_t cap = 0;  // pairs
+  uint64_t cap = 0;  // pairs (device buffers)
+  uint64_t h_pairs_cap = 0, h_out_cap = 0;  // bytes (pinned staging)
   cudaEvent_t done = nullptr;
   bool busy = false;
   QueryReq req{};
@@ -93,6 +94,7 @@ struct dvg_server {
   std::deque<QueryReq> queries;
   std::unordered_map<uint64_t, ServerIndex> indices;
   std::vector<dvg_matrix*> to_free;  // released indices, freed by the build worker
+  std::vector<void*> retired_host;   // outgrown pinned staging, freed at shutdown
   std::deque<dvg_completion> done;
   uint64_t next_id = 1;
   uint64_t resident = 0, reserved = 0;
@@ -211,6 +213,10 @@ void build_worker(dvg_server* s) {
       std::lock_guard<std::mutex> lk(s->mu);
       s->growth = s->bctx->plan_growth;
       s->st.build_batches++;
+      s->st.build_reruns = s->bctx->stats.spgemm_reruns;
+      s->st.build_batch_ns_max = std::max(s->st.build_batch_ns_max, t_done - t_start);
+      s->st.build_alloc_ns = s->bctx->stats.host_alloc_ns;
+      s->st.build_sync_ns = s->bctx->stats.host_sync_ns;
       for (size_t k = 0; k < batch.size(); ++k) {
         ServerIndex& ix = s->indices[batch[k].id];
         s->reserved -= batch[k].predicted;
@@ -244,36 +250,48 @@ void build_worker(dvg_server* s) {
 
 // ---- query worker -------------------------------------------------------------
 
-void ensure_slot(dvg_server* s, QuerySlot& q, uint64_t npairs) {
-  if (npairs <= q.cap) return;
+// Device buffers of a slot grow by doubling (stream-ordered, through the
+// context's cache).  Pinned staging is only made for callers whose buffers
+// are pageable, also by doubling; outgrown pinned buffers are kept until the
+// server shuts down, because cudaFreeHost waits for the whole device and would
+// stall the build stream.
+void ensure_slot(dvg_server* s, QuerySlot& q, uint64_t npairs, bool stage_in, bool stage_out) {
   dvg_context* ctx = s->qctx;
-  const uint64_t cap = std::max<uint64_t>(npairs, 1u << 16);
-  if (q.d_pairs) dvg::dfree(ctx, q.d_pairs);
-  if (q.d_out) dvg::dfree(ctx, q.d_out);
-  if (q.h_pairs) DVG_CUDA(cudaFreeHost(q.h_pairs));
-  if (q.h_out) DVG_CUDA(cudaFreeHost(q.h_out));
-  q.d_pairs = nullptr;
-  q.d_out = nullptr;
-  q.h_pairs = nullptr;
-  q.h_out = nullptr;
-  q.cap = 0;
-  q.d_pairs = static_cast<uint32_t*>(dvg::dalloc(ctx, cap * 8));
-  q.d_out = static_cast<uint8_t*>(dvg::dalloc(ctx, cap));
-  DVG_CUDA(cudaMallocHost(&q.h_pairs, cap * 8));
-  DVG_CUDA(cudaMallocHost(&q.h_out, cap));
-  q.cap = cap;
+  if (npairs > q.cap) {
+    const uint64_t cap = std::max<uint64_t>({npairs, 2 * q.cap, uint64_t(1) << 16});
+    if (q.d_pairs) dvg::dfree(ctx, q.d_pairs);
+    if (q.d_out) dvg::dfree(ctx, q.d_out);
+    q.d_pairs = nullptr;
+    q.d_out = nullptr;
+    q.cap = 0;
+    q.d_pairs = static_cast<uint32_t*>(dvg::dalloc(ctx, cap * 8));
+    q.d_out = static_cast<uint8_t*>(dvg::dalloc(ctx, cap));
+    q.cap = cap;
+  }
+  auto grow_host = [&](void*& h, uint64_t& hcap, uint64_t bytes) {
+    if (bytes <= hcap) return;
+    const uint64_t want = std::max<uint64_t>({bytes, 2 * hcap, uint64_t(1) << 16});
+    void* p = nullptr;
+    DVG_CUDA(cudaMallocHost(&p, want));
+    if (h) s->retired_host.push_back(h);
+    h = p;
+    hcap = want;
+  };
+  if (stage_in) grow_host(reinterpret_cast<void*&>(q.h_pairs), q.h_pairs_cap, npairs * 8);
+  if (stage_out) grow_host(reinterpret_cast<void*&>(q.h_out), q.h_out_cap, npairs);
 }
 
 // Issues one query batch on the query context's stream.
 void issue_query(dvg_server* s, QuerySlot& q, const QueryReq& r, const dvg_matrix* idx) {
   dvg_context* ctx = s->qctx;
-  ensure_slot(s, q, r.npairs);
+  const bool stage_in = r.npairs && !is_pinned(r.pairs);
+  q.staged_out = r.npairs && !is_pinned(r.answers);
+  ensure_slot(s, q, r.npairs, stage_in, q.staged_out);
   const uint32_t* src = r.pairs;
-  if (r.npairs && !is_pinned(r.pairs)) {
+  if (stage_in) {
     std::memcpy(q.h_pairs, r.pairs, r.npairs * 8);
     src = q.h_pairs;
   }
-  q.staged_out = r.npairs && !is_pinned(r.answers);
   uint8_t* dst = q.staged_out ? q.h_out : r.answers;
   DVG_CUDA(cudaMemsetAsync(q.d_ctl, 0, sizeof(DeviceControl), ctx->stream));
   if (r.npairs) {
@@ -411,10 +429,34 @@ dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out) {
   if (st == DVG_OK) st = dvg_init(cfg->device, &s->qctx);
   if (st == DVG_OK) {
     try {
+      // queries run on the device's highest-priority stream: when a build
+      // kernel's CTAs retire, a waiting query kernel is scheduled before the
+      // build's next kernel, so a query waits for one kernel, not a batch
+      int prio_lo = 0, prio_hi = 0;
+      DVG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+      DVG_CUDA(cudaStreamDestroy(s->qctx->own_stream));
+      s->qctx->own_stream = nullptr;
+      DVG_CUDA(cudaStreamCreateWithPriority(&s->qctx->own_stream, cudaStreamNonBlocking, prio_hi));
+      s->qctx->stream = s->qctx->own_stream;
       if (!s->cfg.hbm_budget_bytes) {
         size_t free_b = 0, total_b = 0;
         DVG_CUDA(cudaMemGetInfo(&free_b, &total_b));
         s->cfg.hbm_budget_bytes = uint64_t(0.8 * double(free_b));
+      }
+      // map device memory into the stream-ordered pool now, once: growing the
+      // pool under a build batch costs about 0.2 s per GB, all of it latency
+      // of the requests in the batch.  The pool keeps freed memory (release
+      // threshold at maximum), so later allocations up to this size only
+      // suballocate.
+      {
+        const uint64_t warm = std::min<uint64_t>(s->cfg.hbm_budget_bytes, uint64_t(8) << 30);
+        void* p = nullptr;
+        if (cudaMallocAsync(&p, warm, s->bctx->stream) == cudaSuccess) {
+          DVG_CUDA(cudaFreeAsync(p, s->bctx->stream));
+          DVG_CUDA(cudaStreamSynchronize(s->bctx->stream));
+        } else {
+          (void)cudaGetLastError();
+        }
       }
       s->slots.resize(s->cfg.max_inflight_queries);
       for (auto& q : s->slots) {
@@ -466,6 +508,7 @@ dvg_status dvg_server_destroy(dvg_server* s) {
     if (q.h_ctl) cudaFreeHost(q.h_ctl);
     if (q.done) cudaEventDestroy(q.done);
   }
+  for (void* h : s->retired_host) cudaFreeHost(h);
   dvg_status a = dvg_shutdown(s->qctx), b = dvg_shutdown(s->bctx);
   delete s;
   return a != DVG_OK ? a : b;

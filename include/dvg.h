@@ -263,6 +263,10 @@ typedef struct dvg_server_stats {
   uint64_t resident_bytes;       /* indices held in HBM */
   uint64_t peak_reserved_bytes;  /* most resident + predicted in-flight bytes seen */
   uint64_t hbm_budget_bytes;
+  uint64_t build_reruns;         /* builds whose planned capacity was outgrown: re-run step by step */
+  uint64_t build_batch_ns_max;   /* longest build batch, host clock */
+  uint64_t build_alloc_ns;       /* build worker: host time in device allocation calls */
+  uint64_t build_sync_ns;        /* build worker: host time waiting for its stream */
 } dvg_server_stats;
 
 dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out);
