@@ -44,3 +44,20 @@ def test_init_fails_loudly_without_a_device():
     st = N.lib().dvg_init(0, ctypes.byref(h))
     assert st == N.DEVICE and not h.value
     assert N.lib().dvg_last_error()
+
+
+def header_struct_fields(header, name):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = re.search(r"typedef struct " + name + r"\s*\{(.*?)\}\s*" + name + ";", text, flags=re.S).group(1)
+    return [m.group(1) for m in re.finditer(r"\b(\w+)\s*;", body)]
+
+
+@pytest.mark.parametrize("header,name,cls", [
+    ("dvg.h", "dvg_stats", N.DvgStats), ("dvg.h", "dvg_server_config", N.ServerConfig),
+    ("dvg.h", "dvg_completion", N.Completion), ("dvg.h", "dvg_server_stats", N.ServerStats),
+    ("dvg_gen.h", "dvg_graph_params", N.GraphParams), ("dvg_gen.h", "dvg_graph_stats", N.GraphStats),
+    ("dvg_gen.h", "dvg_host_matrix", N.HostMatrix)])
+def test_ctypes_structs_follow_the_header(header, name, cls):
+    # the Python mirror of each C struct has the header's fields, in order
+    assert [f for f, _ in cls._fields_] == header_struct_fields(header, name)

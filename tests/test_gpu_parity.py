@@ -308,6 +308,33 @@ def test_planned_build_matches_oracle_and_synchronised_path(ctx, window, row_slo
         ctx.set_option("row_slot", 1)
 
 
+@pytest.mark.parametrize("chunk_rows", [0, 2048])
+def test_row_kernel_with_and_without_staged_write_out(ctx, chunk_rows):
+    # deferred write-out through the staging buffers (default) and the chunk
+    # written out in its own iteration give the oracle's index and product;
+    # the banded product has chunks that outgrow the staging (written in
+    # place) next to chunks that fit it
+    set_plan(ctx, (0, 0, 0, 0), chunk_rows)
+    g, _ = gen.graph_adjacency(gen.small_graph_spec(80_000, seed=17))
+    want = orc.dindex(omat(g), 150, 320, algo="hbv")
+    a = gen.banded(30_000, 300, 2.0, 1.0, seed=71)
+    b = gen.banded(30_000, 400, 6.0, 3.0, seed=72)
+    want_ab = orc.spgemm(omat(a), omat(b), algo="hbv")
+    dg = ctx.upload(g)
+    try:
+        for stage in (1, 0):
+            ctx.set_option("row_stage", stage)
+            got = ctx.distance_index(dg, 150, 320).download()
+            assert_same(got, want.rowmap, want.entries, want.nnz, f"stage {stage}")
+            ctx.set_option("spgemm_mode", 2)
+            got = ctx.spgemm(ctx.upload(a), ctx.upload(b)).download()
+            assert_same(got, want_ab.rowmap, want_ab.entries, want_ab.nnz, f"stage {stage}")
+            ctx.set_option("spgemm_mode", 0)
+    finally:
+        ctx.set_option("row_stage", 1)
+        ctx.set_option("spgemm_mode", 0)
+
+
 def test_planned_build_outgrowing_its_estimate_reruns_exactly(ctx):
     # a capacity estimate of nothing: the first step overflows, the later
     # steps stand down, and the build re-runs on the read-back path
