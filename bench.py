@@ -59,7 +59,7 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                    help="a context option (dvg_set_option) for the run; repeatable")
-    p.add_argument("--workload", choices=["build", "batch", "spgemm", "serve"], default="build",
+    p.add_argument("--workload", choices=["build", "batch", "spgemm", "serve", "adjacency"], default="build",
                    help="build: the plain chromosome-scale index build (the headline); batch: 2,000 "
                         "mixed-size graphs in one batched build vs back-to-back single builds; spgemm: "
                         "range_spgemm / range_spadd alone on banded 2^24-row matrices; serve: the "
@@ -338,6 +338,74 @@ def run_batch(args, ctx, stream, rank):
             "autotune_builds": tuned, "sizes_match_plain": bool(same)}
 
 
+def run_adjacency(args, ctx, stream, rank):
+    """Adjacency construction (util::range_adjacency_matrix) of the
+    chromosome-scale synthetic graph, compacted into nodes, on the device:
+    host node lengths and edges in, the range-CRS matrix resident in HBM (the
+    step a build starts from).  e2e adds the download of the matrix to pinned
+    host buffers.  The CPU baseline is the oracle's single-thread restatement
+    of the reference's host construction (adjacency.hpp:170-228 and the
+    Basic->Range append, crs_matrix.hpp:197-242) on the same graph."""
+    import torch
+    from diverg_b200 import gen
+    spec = gen.chromosome_graph_spec(args.n_backbone, seed=args.seed + rank)
+    lens, edges = gen.graph_nodes(spec)
+    nloci = int(lens.sum())
+    for _ in range(args.warmup):
+        ctx.adjacency_from_graph(lens, edges).free()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.reset_stats()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        m = ctx.adjacency_from_graph(lens, edges)
+        nentries, nnz = m.nentries, m.nnz
+        m.free()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    st = ctx.stats()
+    step_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    # algorithmic bytes: node lengths and edges in, rows out
+    out_bytes = 8 * (nloci + 1) + 4 * nentries
+    alg = 4 * len(lens) + 8 * len(edges) + out_bytes
+    # e2e: the same plus the matrix into pinned host memory
+    o_rowmap = torch.empty(nloci + 1, dtype=torch.int64).pin_memory()
+    o_entries = torch.empty(max(1, nentries), dtype=torch.int32).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        m = ctx.adjacency_from_graph(lens, edges)
+        m.download_to(o_rowmap.data_ptr(), o_entries.data_ptr())
+        m.free()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        from oracle import pyoracle as orc
+        t0 = time.perf_counter()
+        ref = orc.adjacency(lens, edges)
+        cpu_s = time.perf_counter() - t0
+        assert len(ref.entries) == nentries
+        cpu = {"value": cpu_s, "unit": "s", "cores": 1, "kind": "port",
+               "sample": f"the whole graph ({nloci} loci), the oracle's single-thread restatement of the "
+                         "reference's host adjacency construction"}
+    peak, peak_kind = peaks()
+    return {"metric": "adjacency construction s", "value": step_s, "unit": "s", "higher_is_better": False,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "range adjacency of the chromosome-scale synthetic graph from its node graph",
+                       "n_backbone": args.n_backbone, "nodes": int(len(lens)), "edges": int(len(edges)),
+                       "loci": nloci, "seed": args.seed},
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(4 * len(lens) + 8 * len(edges)),
+                    "d2h_bytes_per_step": int(out_bytes)},
+            "roofline": {"bound": "hbm", "achieved": alg / step_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / step_s / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "note": "whole call (two read-backs size the output), algorithmic bytes over its time"},
+            "gpu_launches": st["kernel_launches"] / args.steps, "cpu_baseline": cpu,
+            "index": {"entries": int(nentries), "nnz": int(nnz)}}
+
+
 def apply_options(ctx, pairs):
     for kv in pairs:
         key, _, value = kv.partition("=")
@@ -528,6 +596,8 @@ def run_other(args, rank, world, local):
             line = run_spgemm_micro(args, ctx, stream, rank)
         elif args.workload == "batch":
             line = run_batch(args, ctx, stream, rank)
+        elif args.workload == "adjacency":
+            line = run_adjacency(args, ctx, stream, rank)
         else:
             from diverg_b200 import serving
             line = serving.bench_line(args, ctx, rank)

@@ -104,6 +104,7 @@ DVG_SIGNATURES = {
     "dvg_range_power": [_P, _P, ctypes.c_uint, _PP],
     "dvg_create_distance_index": [_P, _P, ctypes.c_uint, ctypes.c_uint, _PP],
     "dvg_batch_distance_index": [_P, _U32, _P, _P, _P, _P],
+    "dvg_adjacency_from_graph": [_P, _U32, _P, ctypes.c_uint64, _P, _U32, _U32, _PP],
     "dvg_query_batch": [_P, _P, _P, _U64, _P],
     "dvg_query_batch_host": [_P, _P, _P, _U64, _P],
     "dvg_range_spgemm_noalloc": [_U32, _U32, _P, _P, _U64, _U32, _U32, _P, _P, _U64, _P, _P, _U64,
@@ -122,6 +123,9 @@ DVG_SIGNATURES = {
 GEN_SIGNATURES = {
     "dvg_gen_graph_adjacency": [ctypes.POINTER(GraphParams), ctypes.POINTER(HostMatrix), ctypes.POINTER(GraphStats)],
     "dvg_gen_graph_edges": [ctypes.POINTER(GraphParams), ctypes.POINTER(_U64), ctypes.POINTER(_U64),
+                            ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32))],
+    "dvg_gen_graph_nodes": [ctypes.POINTER(GraphParams), ctypes.POINTER(_U64),
+                            ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)), ctypes.POINTER(_U64),
                             ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32))],
     "dvg_gen_banded": [_U32, _U32, ctypes.c_double, ctypes.c_double, _U64, ctypes.POINTER(HostMatrix)],
     "dvg_gen_random": [_U32, _U64, _U64, ctypes.POINTER(HostMatrix)],

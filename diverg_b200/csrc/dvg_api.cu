@@ -1045,6 +1045,18 @@ dvg_status dvg_range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k, dv
   });
 }
 
+dvg_status dvg_adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uint32_t* node_len, uint64_t nedges,
+                                    const uint32_t* edges, uint32_t lower, uint32_t upper, dvg_matrix** out) {
+  return guarded([&] {
+    Lock lk(ctx);
+    require(out != nullptr, "null argument");
+    require(nedges == 0 || edges != nullptr, "null edges");
+    for (uint64_t e = 0; e < 2 * nedges; ++e)
+      require(edges[e] >= 1 && edges[e] <= nnodes, "edge endpoint is not a node id in 1..nnodes");
+    *out = adjacency_from_graph(ctx, nnodes, node_len, nedges, edges, lower, upper);
+  });
+}
+
 dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, unsigned dmin, unsigned dmax,
                                      dvg_matrix** out) {
   return guarded([&] {

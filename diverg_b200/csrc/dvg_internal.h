@@ -120,6 +120,10 @@ void record_error(const std::string& msg);
 void* dalloc(dvg_context* ctx, size_t bytes);
 void dfree(dvg_context* ctx, void* p);
 size_t device_free_bytes(dvg_context* ctx);  // free device memory for planning (cached query)
+// The range-CRS adjacency of nodes [lower, upper) of a sequence graph
+// (dvg_adjacency.cu; arguments as dvg_adjacency_from_graph, host arrays).
+dvg_matrix* adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uint32_t* node_len,
+                                 uint64_t nedges, const uint32_t* edges, uint32_t lower, uint32_t upper);
 
 // A device matrix owned by the context's allocator.
 dvg_matrix* new_matrix(dvg_context* ctx, uint32_t nrows, uint32_t ncols, uint64_t nentries);

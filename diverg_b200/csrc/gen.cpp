@@ -247,6 +247,58 @@ int dvg_gen_graph_edges(const dvg_graph_params* gp, uint64_t* n_nodes, uint64_t*
   return 0;
 }
 
+int dvg_gen_graph_nodes(const dvg_graph_params* gp, uint64_t* n_nodes, uint32_t** node_len, uint64_t* n_edges,
+                        uint32_t** edges) {
+  if (!valid(gp) || !n_nodes || !node_len || !n_edges || !edges) return 1;
+  dvg_graph_stats st;
+  std::vector<Event> ev = draw_events(gp, &st);
+  if (st.n_loci >= 0xFFFFFFFEull) return 1;
+  const uint64_t n = st.n_loci;
+  // loci come in topological order, so when locus l is reached every
+  // predecessor of l has been seen and its in-degree is final
+  std::vector<uint8_t> indeg(n, 0);
+  std::vector<uint64_t> starts;
+  std::vector<uint64_t> links;  // inter-node edges as (from locus, to locus)
+  bool have_prev = false;
+  int prev_ns = 0;
+  uint64_t prev_succ = 0;
+  walk_graph(gp, ev, [&](uint64_t l, const uint64_t* succ, int ns) {
+    // l opens a node unless it continues the chain of l - 1
+    if (!have_prev || indeg[l] != 1 || prev_ns != 1 || prev_succ != l) starts.push_back(l);
+    for (int k = 0; k < ns; ++k)
+      if (indeg[succ[k]] < 255) ++indeg[succ[k]];
+    for (int k = 0; k < ns; ++k) {
+      const bool chain = ns == 1 && succ[k] == l + 1 && indeg[succ[k]] == 1;
+      if (!chain) {
+        links.push_back(l);
+        links.push_back(succ[k]);
+      }
+    }
+    have_prev = true;
+    prev_ns = ns;
+    prev_succ = ns ? succ[0] : 0;
+  });
+  const uint64_t m = starts.size();
+  *n_nodes = m;
+  *n_edges = links.size() / 2;
+  *node_len = (uint32_t*)std::malloc(sizeof(uint32_t) * (m ? m : 1));
+  *edges = (uint32_t*)std::malloc(sizeof(uint32_t) * (links.empty() ? 1 : links.size()));
+  if (!*node_len || !*edges) {
+    std::free(*node_len);
+    std::free(*edges);
+    *node_len = nullptr;
+    *edges = nullptr;
+    return 2;
+  }
+  for (uint64_t k = 0; k < m; ++k) (*node_len)[k] = uint32_t((k + 1 < m ? starts[k + 1] : n) - starts[k]);
+  // node id of a locus: the number of node starts at or before it
+  auto node_of = [&](uint64_t x) {
+    return uint32_t(std::upper_bound(starts.begin(), starts.end(), x) - starts.begin());
+  };
+  for (size_t k = 0; k < links.size(); ++k) (*edges)[k] = node_of(links[k]);
+  return 0;
+}
+
 int dvg_gen_banded(uint32_t n, uint32_t hw, double mean_ranges, double mean_len, uint64_t seed,
                    dvg_host_matrix* out) {
   if (!out || n == 0 || n >= 0xFFFFFFFEu || mean_ranges < 0 || mean_len < 1) return 1;

@@ -75,6 +75,25 @@ def graph_edges(spec: GraphSpec):
     return int(nn.value), edges
 
 
+def graph_nodes(spec: GraphSpec):
+    """The synthetic graph with its chains of bases compacted into nodes:
+    (node_len uint32[N] for ids 1..N in rank order, edges uint32[E, 2] of
+    (from_id, to_id)).  Its range adjacency is graph_adjacency(spec)."""
+    nn, ne = ctypes.c_uint64(), ctypes.c_uint64()
+    lp, ep = ctypes.POINTER(ctypes.c_uint32)(), ctypes.POINTER(ctypes.c_uint32)()
+    p = spec.params()
+    rc = N.gen_lib().dvg_gen_graph_nodes(ctypes.byref(p), ctypes.byref(nn), ctypes.byref(lp), ctypes.byref(ne),
+                                         ctypes.byref(ep))
+    if rc:
+        raise ValueError(f"graph generator failed ({rc})")
+    lens = np.ctypeslib.as_array(lp, shape=(nn.value,)).copy() if nn.value else np.zeros(0, np.uint32)
+    edges = np.ctypeslib.as_array(ep, shape=(2 * ne.value,)).copy().reshape(-1, 2) if ne.value else \
+        np.zeros((0, 2), np.uint32)
+    N.gen_lib().dvg_gen_free_ptr(ctypes.cast(lp, ctypes.c_void_p))
+    N.gen_lib().dvg_gen_free_ptr(ctypes.cast(ep, ctypes.c_void_p))
+    return lens, edges
+
+
 def banded(n, half_width=512, mean_ranges=4.0, mean_len=32.0, seed=42) -> CRSMatrix:
     """Random banded matrix, canonical rows (see dvg_gen_banded)."""
     hm = N.HostMatrix()

@@ -113,6 +113,19 @@ class Context:
         N.check(N.lib().dvg_create_distance_index(self.handle, a.handle, dmin, dmax, ctypes.byref(h)))
         return DeviceMatrix(self, h)
 
+    def adjacency_from_graph(self, node_len, edges, lower=1, upper=0) -> "DeviceMatrix":
+        """Range-CRS adjacency of a sequence graph built on the device
+        (dvg_adjacency_from_graph; util::range_adjacency_matrix,
+        adjacency.hpp:249-265).  node_len[id-1] is the length of node id
+        (ids 1..N in rank order); edges is (from_id, to_id) rows; the matrix
+        covers nodes [lower, upper), upper = 0 meaning through the last."""
+        node_len = np.ascontiguousarray(node_len, dtype=np.uint32)
+        edges = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2)
+        h = ctypes.c_void_p()
+        N.check(N.lib().dvg_adjacency_from_graph(self.handle, len(node_len), N.ptr(node_len), len(edges),
+                                                 N.ptr(edges), lower, upper, ctypes.byref(h)))
+        return DeviceMatrix(self, h)
+
     def batch_distance_index(self, graphs, windows):
         """Indices of many independent graphs (DeviceMatrix list) with their
         (dmin, dmax) windows, built in one pass (dvg_batch_distance_index)."""

@@ -180,6 +180,28 @@ dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, uns
 dvg_status dvg_batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* const* graphs,
                                     const unsigned* dmin, const unsigned* dmax, dvg_matrix** out);
 
+/* ---- adjacency construction: util::range_adjacency_matrix
+ *      (adjacency.hpp:249-265) over util::adjacency_matrix (:170-228) and the
+ *      Basic->Range conversion of crs_matrix::append (crs_matrix.hpp:197-242)
+ *
+ * The range-CRS adjacency matrix of a sequence graph, built on the device.
+ * Nodes have ids 1..nnodes in rank order; node_len[id-1] is the length of
+ * node id in bases (at least 1); edges[2k], edges[2k+1] = (from_id, to_id),
+ * in any order, repeats allowed.  The matrix covers the nodes lower .. upper-1
+ * (upper = 0: through the last node; lower = 1 and upper = 0 is the whole
+ * graph, the reference's defaults): one row and column per base, numbered in
+ * rank order from the first base of node `lower`; each base links to the next
+ * base of its node, a node's last base to the first base of every successor,
+ * columns sorted, then rows turned into ranges as append does (a column
+ * extends the open range only if it is the range's end + 1, so a repeated
+ * edge gives a repeated range and a non-canonical matrix).  nnz is the number
+ * of Basic entries, (bases - nodes) + edges.  Edges whose source lies outside
+ * the range are ignored; an edge from inside to outside the range is
+ * DVG_ERR_INVALID_ARG (the reference requires the range to be closed, its
+ * components).  More than 2^32 - 2 bases is DVG_ERR_OVERFLOW. */
+dvg_status dvg_adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uint32_t* node_len, uint64_t nedges,
+                                    const uint32_t* edges, uint32_t lower, uint32_t upper, dvg_matrix** out);
+
 /* ---- range SpGEMM without device allocation -------------------------------
  * No counterpart in the reference.  Some callers of this library cannot let it
  * allocate device memory: a server that reserves the GPU's memory for resident

@@ -79,6 +79,17 @@ int dvg_gen_graph_adjacency(const dvg_graph_params* p, dvg_host_matrix* out, dvg
  * (from_id, to_id).  Used to cross-check the adjacency layout. */
 int dvg_gen_graph_edges(const dvg_graph_params* p, uint64_t* n_nodes, uint64_t* n_edges, uint32_t** edges);
 
+/* The same graph with its chains of bases compacted into nodes: a base
+ * starts a node unless its only predecessor is the previous base and that
+ * base's only successor is it.  Node ids are 1-based in base order (rank
+ * order), node_len[id-1] bases each; edges[2k], edges[2k+1] = (from_id,
+ * to_id) link a node's last base to a successor's first base.  The range
+ * adjacency of this node graph (util::range_adjacency_matrix,
+ * adjacency.hpp:249-265) is the matrix of dvg_gen_graph_adjacency.  Release
+ * both arrays with dvg_gen_free_ptr. */
+int dvg_gen_graph_nodes(const dvg_graph_params* p, uint64_t* n_nodes, uint32_t** node_len, uint64_t* n_edges,
+                        uint32_t** edges);
+
 /* Random banded matrix: row i holds Poisson(mean_ranges) ranges whose starts
  * are uniform in [i-half_width, i+half_width] and whose lengths are geometric
  * with mean mean_len; ranges are clipped to the band and to [0,n), sorted and

@@ -40,6 +40,9 @@ typedef struct orc_mat {
   uint32_t* entries;  /* nentries */
 } orc_mat;
 
+orc_mat* orc_adjacency_range(uint32_t nnodes, const uint32_t* node_len, uint64_t nedges, const uint32_t* edges,
+                             uint32_t lower, uint32_t upper);
+
 }  // extern "C"
 
 namespace {
@@ -397,24 +400,36 @@ orc_mat* orc_basic_to_range(uint32_t nrows, uint32_t ncols, const uint64_t* rowm
  * matrix is then converted to range CRS (adjacency.hpp:249-265).
  * edges are (src_id, dst_id) pairs, ids 1-based. */
 orc_mat* orc_adjacency(uint32_t nnodes, const uint32_t* node_len, uint64_t nedges, const uint32_t* edges) {
+  return orc_adjacency_range(nnodes, node_len, nedges, edges, 1, 0);
+}
+
+/* The same for the nodes lower .. upper-1 (upper = 0: through the last node),
+ * as adjacency_matrix(graph, lower, upper): loci numbered from the first
+ * locus of node `lower` (id_to_charorder(to) - start, adjacency.hpp:205,220),
+ * only the edges out of nodes in the range (for_each_node from `lower`,
+ * stopping after rank upper-1, :209-226). */
+orc_mat* orc_adjacency_range(uint32_t nnodes, const uint32_t* node_len, uint64_t nedges, const uint32_t* edges,
+                             uint32_t lower, uint32_t upper) {
+  if (upper == 0) upper = nnodes + 1;
   std::vector<uint64_t> charorder(size_t(nnodes) + 2, 0);
   for (uint32_t id = 1; id <= nnodes; ++id) charorder[id + 1] = charorder[id] + node_len[id - 1];
   std::vector<std::vector<uint32_t>> succ(size_t(nnodes) + 1);
   for (uint64_t e = 0; e < nedges; ++e) succ[edges[2 * e]].push_back(edges[2 * e + 1]);
-  uint64_t nloci = charorder[nnodes + 1];
+  const uint64_t start = charorder[lower];
+  const uint64_t nloci = charorder[upper] - start;
   std::vector<uint64_t> rowmap;
   std::vector<uint32_t> cols;
   rowmap.reserve(nloci + 1);
   rowmap.push_back(0);
   uint64_t cursor = 0;
-  for (uint32_t id = 1; id <= nnodes; ++id) {
+  for (uint32_t id = lower; id < upper; ++id) {
     for (uint32_t off = 1; off < node_len[id - 1]; ++off) {
       cols.push_back(uint32_t(++cursor));
       rowmap.push_back(cols.size());
     }
     ++cursor;
     size_t row_begin = cols.size();
-    for (uint32_t to : succ[id]) cols.push_back(uint32_t(charorder[to]));
+    for (uint32_t to : succ[id]) cols.push_back(uint32_t(charorder[to] - start));
     std::sort(cols.begin() + row_begin, cols.end());
     rowmap.push_back(cols.size());
   }

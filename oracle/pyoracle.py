@@ -67,6 +67,9 @@ def lib():
         L.orc_basic_to_range.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_adjacency.restype = P
         L.orc_adjacency.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_adjacency_range.restype = P
+        L.orc_adjacency_range.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                          ctypes.c_uint32, ctypes.c_uint32]
         L.orc_nnz.restype = ctypes.c_uint64
         L.orc_nnz.argtypes = [P]
         L.orc_max_threads.restype = ctypes.c_int
@@ -147,12 +150,14 @@ def basic_to_range(nrows: int, ncols: int, rowmap: np.ndarray, cols: np.ndarray)
     return _take(lib().orc_basic_to_range(nrows, ncols, rowmap.ctypes.data, cols.ctypes.data))
 
 
-def adjacency(node_len: np.ndarray, edges: np.ndarray) -> OMat:
+def adjacency(node_len: np.ndarray, edges: np.ndarray, lower: int = 1, upper: int = 0) -> OMat:
     """util::range_adjacency_matrix (adjacency.hpp:170-265); node ids 1..N in
-    rank order, edges as (from_id, to_id) rows."""
+    rank order, edges as (from_id, to_id) rows, the nodes [lower, upper)
+    (upper = 0: through the last node)."""
     node_len = np.ascontiguousarray(node_len, dtype=np.uint32)
     edges = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2)
-    return _take(lib().orc_adjacency(len(node_len), node_len.ctypes.data, len(edges), edges.ctypes.data))
+    return _take(lib().orc_adjacency_range(len(node_len), node_len.ctypes.data, len(edges), edges.ctypes.data,
+                                           lower, upper))
 
 
 def nnz(m) -> int:
