@@ -10,6 +10,7 @@
 #include <stdexcept>
 #include <vector>
 
+#include <diverg/adjacency.hpp>
 #include <diverg/dindex_eti.hpp>
 #include <dvg_gen.h>
 
@@ -30,6 +31,31 @@ void orc_mat_free(orc_mat* m);
 
 using RCRS = diverg::CRSMatrix<diverg::crs_matrix::RangeDynamic, bool, uint32_t, uint64_t>;
 using RCRS32 = diverg::CRSMatrix<diverg::crs_matrix::RangeDynamic, bool, uint32_t, uint32_t>;
+
+// The part of gum's SeqGraph interface util::range_adjacency_matrix walks
+// (adjacency.hpp:170-228), over a node list; ids differ from ranks
+// (id = 3 rank + 7) so the rank conversion is exercised.
+struct NodeGraph {
+  typedef uint64_t id_type;
+  typedef uint64_t rank_type;
+  typedef int linktype_type;
+  std::vector<uint32_t> len;                // by rank - 1
+  std::vector<std::vector<uint64_t>> out;   // successor ranks, by rank - 1
+  rank_type get_node_count() const { return len.size(); }
+  id_type rank_to_id(rank_type r) const { return 3 * r + 7; }
+  rank_type id_to_rank(id_type id) const { return (id - 7) / 3; }
+  uint64_t node_length(id_type id) const { return len[id_to_rank(id) - 1]; }
+  template <class F>
+  void for_each_node(F f, rank_type from = 1) const {
+    for (rank_type r = from; r <= len.size(); ++r)
+      if (!f(r, rank_to_id(r))) return;
+  }
+  template <class F>
+  void for_each_edges_out(id_type id, F f) const {
+    for (uint64_t to : out[id_to_rank(id) - 1])
+      if (!f(rank_to_id(to), 0)) return;
+  }
+};
 
 static int failures = 0;
 #define CHECK(cond)                                                   \
@@ -121,6 +147,29 @@ int main() {
   back.load(ss);
   CHECK(back.get_rowmap() == eti.get_rowmap() && back.get_entries() == eti.get_entries() &&
         back.nnz() == eti.nnz() && back.numCols() == eti.numCols());
+
+  // adjacency of the node graph == the generator's adjacency (adjacency.hpp:249-265)
+  {
+    uint64_t nn = 0, ne = 0;
+    uint32_t *lens = nullptr, *edges = nullptr;
+    CHECK(dvg_gen_graph_nodes(&gp, &nn, &lens, &ne, &edges) == 0);
+    NodeGraph g;
+    g.len.assign(lens, lens + nn);
+    g.out.resize(nn);
+    for (uint64_t e = 0; e < ne; ++e) g.out[edges[2 * e] - 1].push_back(edges[2 * e + 1]);
+    dvg_gen_free_ptr(lens);
+    dvg_gen_free_ptr(edges);
+    RCRS adj = diverg::util::range_adjacency_matrix<RCRS>(g);
+    CHECK(adj.get_rowmap() == ra.get_rowmap() && adj.get_entries() == ra.get_entries() && adj.nnz() == ra.nnz());
+    // the graph is one component: ranks [1, 3) leave an edge behind, which throws
+    threw = false;
+    try {
+      diverg::util::range_adjacency_matrix<RCRS>(g, 1, 3);
+    } catch (std::runtime_error const&) {
+      threw = true;
+    }
+    CHECK(threw);
+  }
 
   // invalid window: the reference aborts, the B200 path throws
   threw = false;
