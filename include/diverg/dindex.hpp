@@ -15,6 +15,7 @@
 #define DIVERG_B200_DINDEX_HPP__
 
 #include <chrono>
+#include <stdexcept>
 
 #include "range_sparse.hpp"
 
@@ -45,6 +46,26 @@ namespace diverg {
       if ( timer1_ptr ) timer1_ptr->reset();
       detail::check( dvg_create_distance_index( detail::context(), da.get(), dlo, dup, dd.out() ) );
       return detail::download< TRCRSMatrix >( dd );
+    }
+
+    /** dindex.hpp:556-570 (dispatching to :435-469): two distance indices of
+     *  the same graph merge into their union A + B, which the reference
+     *  computes with range_spadd for in-core range matrices, as here on the
+     *  device.  The result is a mutable (RangeDynamic) matrix. */
+    template< typename TMutableCRSMatrix, typename TCRSMatrix >
+    inline TMutableCRSMatrix
+    merge_distance_index( TCRSMatrix& dindex1, TCRSMatrix& dindex2 )
+    {
+      static_assert( crs_matrix::is_range_crs_matrix< TCRSMatrix >::value
+                         && crs_matrix::is_range_crs_matrix< TMutableCRSMatrix >::value,
+                     "input and output distance indices must be in the same (Range) group" );
+      if ( dindex1.numRows() != dindex2.numRows() || dindex1.numCols() != dindex2.numCols() )
+        throw std::runtime_error( "diverg: merge_distance_index: the indices differ in shape" );
+      detail::DeviceMatrix d1, d2, dm;
+      detail::upload( dindex1, d1 );
+      detail::upload( dindex2, d2 );
+      detail::check( dvg_range_spadd( detail::context(), d1.get(), d2.get(), dm.out() ) );
+      return detail::download< TMutableCRSMatrix >( dm );
     }
   }  // namespace util
 }  // namespace diverg

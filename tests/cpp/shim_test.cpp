@@ -148,6 +148,16 @@ int main() {
   CHECK(back.get_rowmap() == eti.get_rowmap() && back.get_entries() == eti.get_entries() &&
         back.nnz() == eti.nnz() && back.numCols() == eti.numCols());
 
+  // merging two indices of one graph is their union (dindex.hpp:556-570)
+  {
+    RCRS near = diverg::util::create_distance_index(ra, 1, 3);
+    RCRS far = diverg::util::create_distance_index(ra, 100, 300);
+    RCRS merged = diverg::util::merge_distance_index<RCRS>(near, far);
+    orc_mat vn = view(near), vf = view(far);
+    CHECK(same(merged, orc_spadd(&vn, &vf)));
+    CHECK(merged.nnz() >= far.nnz() && merged.nnz() >= near.nnz());
+  }
+
   // adjacency of the node graph == the generator's adjacency (adjacency.hpp:249-265)
   {
     uint64_t nn = 0, ne = 0;
