@@ -105,6 +105,7 @@ DVG_SIGNATURES = {
     "dvg_create_distance_index": [_P, _P, ctypes.c_uint, ctypes.c_uint, _PP],
     "dvg_batch_distance_index": [_P, _U32, _P, _P, _P, _P],
     "dvg_adjacency_from_graph": [_P, _U32, _P, ctypes.c_uint64, _P, _U32, _U32, _PP],
+    "dvg_selftest_bounded_wait": [_P, _U32],
     "dvg_query_batch": [_P, _P, _P, _U64, _P],
     "dvg_query_batch_host": [_P, _P, _P, _U64, _P],
     "dvg_range_spgemm_noalloc": [_U32, _U32, _P, _P, _U64, _U32, _U32, _P, _P, _U64, _P, _P, _U64,

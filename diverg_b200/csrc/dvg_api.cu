@@ -1045,6 +1045,17 @@ dvg_status dvg_range_power(dvg_context* ctx, const dvg_matrix* a, unsigned k, dv
   });
 }
 
+dvg_status dvg_selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit) {
+  return guarded([&] {
+    Lock lk(ctx);
+    reset_control(ctx);
+    selftest_bounded_wait(ctx, spin_limit);
+    const DeviceControl c = read_control(ctx);
+    if (c.timeout) throw Error(DVG_ERR_TIMEOUT, "self-test: the look-back wait ran out, as it must");
+    throw Error(DVG_ERR_DEVICE, "self-test: a wait on a chunk nothing publishes returned without a timeout");
+  });
+}
+
 dvg_status dvg_adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uint32_t* node_len, uint64_t nedges,
                                     const uint32_t* edges, uint32_t lower, uint32_t upper, dvg_matrix** out) {
   return guarded([&] {

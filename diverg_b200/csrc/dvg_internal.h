@@ -218,6 +218,10 @@ struct RowLaunchShape {
 RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_rows_opt, int slot_variant);
 void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& shape);
 int row_slot_entries(int variant);
+// Runs the row kernel's look-back on descriptors nothing publishes, its wait
+// bounded by spin_limit polls (the kernel records a timeout in the control
+// block and returns).
+void selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit);
 
 // Host orchestration (dvg_api.cu).
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b);

@@ -75,6 +75,8 @@ struct FusedArgs {
   // every chunk is written out in its own iteration
   uint32_t* stage_buf;
   uint32_t stage_cap;
+  // polls a look-back waits before it gives up (0: kSpinLimit)
+  uint32_t spin_limit;
 };
 
 // Row `row` of the (shifted) identity: column row + a_shift, or an empty

@@ -159,7 +159,7 @@ __device__ unsigned long long lookback_block(RowSmem<SLOT>& S, const FusedArgs& 
     }
     par ^= 1u;
     if (wait) {  // a chunk after the nearest prefix has published nothing yet
-      if (++spins > kSpinLimit) {
+      if (++spins > (p.spin_limit ? p.spin_limit : kSpinLimit)) {
         if (tid == 0) raise_flag(p, &p.ctl->timeout, 1ull);
         break;
       }
@@ -665,6 +665,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   }
 }
 
+// One CTA runs the look-back of chunk t over descriptors nothing publishes,
+// so its bounded wait must run out (the library's self-test of that path).
+__global__ void __launch_bounds__(kThreads, 1) k_lookback_selftest(FusedArgs p, uint32_t t) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RowSmem<16>& S = *reinterpret_cast<RowSmem<16>*>(smem_raw);
+  uint32_t par = 0;
+  (void)lookback_block(S, p, t, 0ull, par);
+}
+
 template <bool A_ID, int SLOT>
 struct RowKernel {
   static void* get() { return reinterpret_cast<void*>(&k_spgemm_rowmode<A_ID, SLOT>); }
@@ -705,6 +714,29 @@ RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_
   s.desc_bytes = size_t(s.nchunks) * sizeof(ChunkDesc);
   s.stage_bytes = size_t(s.grid) * 2 * (kRowStagePerRow + 1) * s.chunk_rows * sizeof(uint32_t);
   return s;
+}
+
+void selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit) {
+  // two descriptors, both empty: chunk 1 waits on chunk 0 for good
+  void* desc = dalloc(ctx, 2 * sizeof(ChunkDesc));
+  try {
+    DVG_CUDA(cudaMemsetAsync(desc, 0, 2 * sizeof(ChunkDesc), ctx->stream));
+    FusedArgs p{};
+    p.desc = static_cast<ChunkDesc*>(desc);
+    p.ctl = ctx->d_ctl;
+    p.nchunks = 2;
+    p.cap = ~0ull;
+    p.spin_limit = spin_limit ? spin_limit : 1;
+    const int smem = int(sizeof(RowSmem<16>));
+    DVG_CUDA(cudaFuncSetAttribute(k_lookback_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_lookback_selftest<<<1, kThreads, smem, ctx->stream>>>(p, 1u);
+    DVG_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
+  } catch (...) {
+    dfree(ctx, desc);
+    throw;
+  }
+  dfree(ctx, desc);
 }
 
 void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& s) {

@@ -180,6 +180,16 @@ dvg_status dvg_create_distance_index(dvg_context* ctx, const dvg_matrix* ra, uns
 dvg_status dvg_batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* const* graphs,
                                     const unsigned* dmin, const unsigned* dmax, dvg_matrix** out);
 
+/* ---- self-test of the bounded device waits
+ *
+ * Every device-side wait of the library (the chunk look-backs of the SpGEMM
+ * kernels) gives up after a bounded number of polls, records a timeout the
+ * host turns into DVG_ERR_TIMEOUT, and leaves the context usable.  This runs
+ * the row kernel's look-back on a chunk whose predecessor nothing publishes,
+ * with the wait bounded by spin_limit polls (0: 1 poll), and returns that
+ * DVG_ERR_TIMEOUT; any other status means the bound did not hold. */
+dvg_status dvg_selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit);
+
 /* ---- adjacency construction: util::range_adjacency_matrix
  *      (adjacency.hpp:249-265) over util::adjacency_matrix (:170-228) and the
  *      Basic->Range conversion of crs_matrix::append (crs_matrix.hpp:197-242)

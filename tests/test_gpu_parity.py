@@ -431,6 +431,18 @@ def test_errors_are_reported(ctx):
         ctx.upload(odd)
 
 
+def test_bounded_device_wait_runs_out_and_the_context_stays_usable(ctx):
+    # a look-back on a chunk whose predecessor nothing publishes: the wait
+    # gives up after its bound, the call reports a timeout, and the same
+    # context computes correctly afterwards (no fault, no hang)
+    for limit in (1, 1000, 20000):
+        assert N.lib().dvg_selftest_bounded_wait(ctx.handle, limit) == N.TIMEOUT
+    a = gen.random_matrix(3000, 9000, seed=5)
+    want = orc.spgemm(omat(a), omat(a), algo="hbv")
+    got = ctx.spgemm(ctx.upload(a), ctx.upload(a)).download()
+    assert_same(got, want.rowmap, want.entries, want.nnz)
+
+
 def test_reference_api_mirror():
     import diverg_b200 as dv
     with dv.ScopedRuntime():
