@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       uint32_t pos = 0;
       // rows that miss the slot wait for the warp-cooperative pass below, so
       // one wide row never holds a whole chunk behind a single thread
-#pragma unroll
+#pragma unroll 1
       for (int u = 0; u < kRowRowsMax; ++u) {
         if (uint32_t(u) >= rpt) break;
         const uint32_t r = (warp * rpt + u) * 32 + lane;
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         if (tid == 0) publish_aggregate(p, t, cnt);
         for (uint32_t r = tid; r < crows; r += kThreads) img[p.stage_cap + r] = incl[r];
         uint32_t spos = 0;
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < kRowRowsMax; ++u) {
           if (uint32_t(u) >= rpt) break;
           const uint32_t r = (warp * rpt + u) * 32 + lane;
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
           if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
         }
         if (nslow_all > uint32_t(kSlowMax)) {
-#pragma unroll
+#pragma unroll 1
           for (int u = 0; u < kRowRowsMax; ++u) {
             if (uint32_t(u) >= rpt) break;
             const uint32_t r = (warp * rpt + u) * 32 + lane;
@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + incl[r];
       if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
       uint32_t pos = 0;
-#pragma unroll
+#pragma unroll 1
       for (int u = 0; u < kRowRowsMax; ++u) {
         if (uint32_t(u) >= rpt) break;
         const uint32_t r = (warp * rpt + u) * 32 + lane;
@@ -619,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
       }
       if (nslow_all > uint32_t(kSlowMax)) {
-#pragma unroll
+#pragma unroll 1
         for (int u = 0; u < kRowRowsMax; ++u) {
           if (uint32_t(u) >= rpt) break;
           const uint32_t r = (warp * rpt + u) * 32 + lane;
