@@ -39,8 +39,8 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per C row of the row kernel, mean of the four
 # launches of profiles/k_spgemm_rowmode_index_1e7.md (ncu, 10,019,292-row
 # graph): traffic scales with the rows of the product
-ROWMODE_TRAFFIC_BYTES_PER_ROW = (485766656 + 323889664 + 329825792 + 327297024 +
-                                 154642944 + 139796480 + 150942464 + 137347328) / 4 / 10019292
+ROWMODE_TRAFFIC_BYTES_PER_ROW = (484378624 + 322835712 + 326777600 + 326171904 +
+                                 151278848 + 137007360 + 143394304 + 133862656) / 4 / 10019292
 
 
 def parse_args():
