@@ -37,7 +37,7 @@ sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per C row of the row kernel, mean of the four
-# launches of profiles/k_spgemm_rowmode_index_1e7.md (ncu, 10,019,292-row
+# launches of the row kernel's ncu capture under profiles/ (10,019,292-row
 # graph): traffic scales with the rows of the product
 ROWMODE_TRAFFIC_BYTES_PER_ROW = (484378624 + 322835712 + 326777600 + 326171904 +
                                  151278848 + 137007360 + 143394304 + 133862656) / 4 / 10019292
@@ -530,7 +530,7 @@ def main():
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": ROWMODE_TRAFFIC_BYTES_PER_ROW * n_loci,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                  "profiles/k_spgemm_rowmode_index_1e7.md, scaled by rows",
+                                  "the row kernel's capture on the 1e7-base graph (profiles/), scaled by rows",
                 "peak_kind": peak_kind,
                 "kernel": "k_spgemm_rowmode (single-pass range SpGEMM: counts, chunk look-back, runs)",
                 "alg_bytes_per_product": per_product_bytes, "products_per_build": st["spgemm_calls"] / args.steps}
