@@ -89,9 +89,17 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// A descriptor word (flag | value) for other CTAs' look-backs.  The word is
+// all a reader takes from it -- no other data of the writer is read on its
+// strength -- so a relaxed store does: a release would first wait for every
+// earlier store of the thread (its share of a chunk image) to land.
+__device__ __forceinline__ void st_relaxed(unsigned long long* q, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(q), "l"(v) : "memory");
+}
+
 // Publishes chunk t's aggregate (its entries) for later chunks' look-backs.
 __device__ __forceinline__ void publish_aggregate(const FusedArgs& p, uint32_t t, unsigned long long cnt) {
-  st_release(&p.desc[t].agg, kFlag | cnt);
+  st_relaxed(&p.desc[t].agg, kFlag | cnt);
 }
 
 // The whole CTA walks back from chunk t (whose aggregate is published),
@@ -171,7 +179,7 @@ __device__ unsigned long long lookback_block(RowSmem<SLOT>& S, const FusedArgs& 
     j -= kThreads;
   }
   if (tid == 0) {
-    st_release(&d[t].incl, kFlag | (pre + cnt));
+    st_relaxed(&d[t].incl, kFlag | (pre + cnt));
     if (t == p.nchunks - 1) {
       p.ctl->total = pre + cnt;
       if (pre + cnt > p.cap) raise_flag(p, &p.ctl->overflow, pre + cnt);
