@@ -663,11 +663,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       S.nslow = 0;
     }
     cta_sync();
-    if (tid == 0) {
-      bool same = true;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) same = same && S.phase[w] == iter;
-      if (!same) raise_flag(p, &p.ctl->status, 64ull);
+    if (warp == 0) {  // one read per lane, one vote
+      const bool off = lane < kWarps && S.phase[lane] != iter;
+      if (__any_sync(kFullMask, off) && lane == 0) raise_flag(p, &p.ctl->status, 64ull);
     }
     t = S.next;
   }
