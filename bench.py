@@ -39,8 +39,8 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per C row of the row kernel, mean of the four
 # launches of the row kernel's ncu capture under profiles/ (10,019,292-row
 # graph): traffic scales with the rows of the product
-ROWMODE_TRAFFIC_BYTES_PER_ROW = (484279808 + 322918144 + 326750208 + 326171904 +
-                                 150806528 + 137545728 + 143506176 + 135797248) / 4 / 10019292
+ROWMODE_TRAFFIC_BYTES_PER_ROW = (484213760 + 322915584 + 327040000 + 326183936 +
+                                 150529280 + 137050368 + 143670272 + 134789632) / 4 / 10019292
 
 
 def parse_args():
