@@ -15,11 +15,18 @@ mean 4 capped at 50, 0.1 % of bubbles structural with length 100..2000, seed
            algorithmic bytes per product (read A and B once, write C once) / its
            mean duration, from CUDA-event spans around every launch in a second,
            instrumented repetition of the timed builds
-  cpu_baseline the CPU restatement of the reference's bitvector SpGEMM path
-           (OpenMP, all host threads) on a prefix of the same graph, scaled
+  cpu_baseline the CPU restatement of the reference's bitvector SpGEMM path and
+           index schedule (OpenMP, all host threads), one build of the whole
+           graph; its index is also the oracle the GPU index is compared with
+           ("parity": every rowmap word, entry and the nnz equal)
+  secondary (N = 1) the other workloads, each with its own clock samples:
+           membership queries against the resident index, the range-SpGEMM /
+           SpAdd kernel microbenchmark, batched builds of 2,000 graphs, and the
+           serving loop under Poisson arrivals
 
 --impl reference times that CPU restatement alone (the reference's own
-Kokkos/OpenMP build cannot be compiled: its submodules are absent).
+Kokkos/OpenMP build cannot be compiled: its submodules are absent), one build
+of the whole graph per timed step.
 With N GPUs each rank builds its own graph (seed 42 + rank): the index is
 block-diagonal over independent components, so ranks share no data.
 """
@@ -36,11 +43,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 2**20
 # DRAM bytes (read + write) per C row of the row kernel, mean of the four
 # launches of the row kernel's ncu capture under profiles/ (10,019,292-row
 # graph): traffic scales with the rows of the product
 ROWMODE_TRAFFIC_BYTES_PER_ROW = (484213760 + 322915584 + 327040000 + 326183936 +
                                  150529280 + 137050368 + 143670272 + 134789632) / 4 / 10019292
+QUERY_ALG_BYTES = 33  # pair 8 B, two rowmap words 16 B, one range 8 B, answer 1 B
 
 
 def parse_args():
@@ -53,20 +62,22 @@ def parse_args():
     p.add_argument("--dmin", type=int, default=400)
     p.add_argument("--dmax", type=int, default=600)
     p.add_argument("--seed", type=int, default=42)
-    p.add_argument("--cpu-target-s", type=float, default=12.0,
-                   help="wall seconds the CPU baseline sample should take")
-    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true",
+                   help="skip the CPU build of the whole graph (and with it the parity check)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-secondary", action="store_true", help="headline build only")
     p.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                    help="a context option (dvg_set_option) for the run; repeatable")
-    p.add_argument("--workload", choices=["build", "batch", "spgemm", "serve", "adjacency"], default="build",
-                   help="build: the plain chromosome-scale index build (the headline); batch: 2,000 "
-                        "mixed-size graphs in one batched build vs back-to-back single builds; spgemm: "
-                        "range_spgemm / range_spadd alone on banded 2^24-row matrices; serve: the "
-                        "request loop under Poisson arrivals")
+    p.add_argument("--workload", choices=["build", "batch", "spgemm", "serve", "adjacency", "query"],
+                   default="build",
+                   help="build: the plain chromosome-scale index build (the headline) followed by the "
+                        "secondary workloads; batch: 2,000 mixed-size graphs in one batched build vs "
+                        "back-to-back single builds; spgemm: range_spgemm / range_spadd alone on banded "
+                        "2^24-row matrices; serve: the request loop under Poisson arrivals; query: membership "
+                        "queries against the resident chromosome-scale index")
     p.add_argument("--graphs", type=int, default=2000, help="batch: number of graphs")
     p.add_argument("--rate", type=float, default=0.0, help="serve: arrivals per second (0: sweep)")
-    p.add_argument("--requests", type=int, default=2000, help="serve: requests per rate")
+    p.add_argument("--requests", type=int, default=1000, help="serve: requests per rate")
     return p.parse_args()
 
 
@@ -139,62 +150,60 @@ def graph(n_backbone, seed):
     return gen.graph_adjacency(spec)
 
 
-def cpu_build_seconds(n_backbone, seed, dmin, dmax):
-    """One index build by the CPU restatement (bitvector SpGEMM, OpenMP)."""
+def omat(m):
     from oracle import pyoracle as orc
-    a, _ = graph(n_backbone, seed)
-    oa = orc.OMat(a.numRows(), a.numCols(), a.rowmap, a.entries, a.nnz())
+    import numpy as np
+    return orc.OMat(m.numRows(), m.numCols(), np.asarray(m.rowmap, dtype=np.uint64), m.entries, m.nnz())
+
+
+def cpu_build(a, dmin, dmax):
+    """One index build of `a` by the CPU restatement of the reference's path
+    (bitvector SpGEMM, the reference's squaring schedule, OpenMP on every host
+    thread): (seconds, the index)."""
+    from oracle import pyoracle as orc
+    oa = omat(a)
     t = time.perf_counter()
-    orc.dindex(oa, dmin, dmax, algo="hbv")
-    return time.perf_counter() - t, a.numRows()
+    idx = orc.dindex(oa, dmin, dmax, algo="hbv")
+    return time.perf_counter() - t, idx
 
 
-def cpu_sample_plan(args, n_full_loci):
-    """Prefix size whose CPU build takes about args.cpu_target_s seconds."""
-    t1, loci1 = cpu_build_seconds(1_000_000, args.seed, args.dmin, args.dmax)
-    per_locus = t1 / loci1
-    n_sample = int(min(args.n_backbone, max(1_000_000, args.cpu_target_s / per_locus)))
-    return n_sample
-
-
-def cpu_baseline(args, n_full_loci):
-    from oracle import pyoracle as orc
-    n_sample = cpu_sample_plan(args, n_full_loci)
-    t, loci = cpu_build_seconds(n_sample, args.seed, args.dmin, args.dmax)
-    scaled = t * n_full_loci / loci
-    return {"value": scaled, "unit": "s", "cores": orc.threads(), "kind": "port",
-            "sample": f"index build [{args.dmin},{args.dmax}] of the first {n_sample:.3g} backbone bases "
-                      f"({loci} loci) of the same graph generator, {t:.2f} s, scaled x{n_full_loci / loci:.1f} "
-                      f"to {n_full_loci} loci; CPU restatement of the reference's bitvector SpGEMM path "
-                      f"(OpenMP, {orc.threads()} threads), not the reference binary"}
+def cpu_kind_note():
+    return ("CPU restatement (OpenMP) of the reference's bitvector SpGEMM path and index schedule, not the reference "
+            "binary: the reference's Kokkos build cannot be compiled here")
 
 
 def run_reference(args, rank, world):
-    """CPU arm: the restated reference path on the host cores, rank 0 only."""
+    """CPU arm: the restated reference path on the host cores, rank 0 only.
+    Every timed step builds the index of the whole graph; warm-up steps build
+    the index of a 1e6-base prefix of the same generator (they only start the
+    thread pool and the allocator)."""
     if rank != 0:
         return
     from oracle import pyoracle as orc
-    from diverg_b200 import gen
-    spec = gen.chromosome_graph_spec(args.n_backbone, seed=args.seed)
-    _, st = gen.graph_adjacency(spec)
-    n_full = st["n_loci"]
-    n_sample = cpu_sample_plan(args, n_full)
+    a, _ = graph(args.n_backbone, args.seed)
+    n_full = a.numRows()
+    warm_backbone = min(args.n_backbone, 1_000_000)
+    aw, _ = graph(warm_backbone, args.seed)
+    for _ in range(args.warmup):
+        cpu_build(aw, args.dmin, args.dmax)
     times = []
-    loci = None
-    for i in range(args.warmup + args.steps):
-        t, loci = cpu_build_seconds(n_sample, args.seed, args.dmin, args.dmax)
-        if i >= args.warmup:
-            times.append(t * n_full / loci)
+    entries = None
+    for _ in range(args.steps):
+        t, idx = cpu_build(a, args.dmin, args.dmax)
+        times.append(t)
+        entries = int(idx.rowmap[-1])
+        del idx
     value = sum(times) / len(times)
+    sample = (f"each timed step: one index build [{args.dmin},{args.dmax}] of the whole graph ({n_full} loci, "
+              f"{entries // 2} index ranges), no scaling; warm-up steps: a {warm_backbone}-base prefix; "
+              + cpu_kind_note())
     line = {
         "impl": "reference", "metric": "index-build s", "value": value, "unit": "s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": config_dict(args, n_full),
-        "cpu_baseline": {"value": value, "unit": "s", "cores": orc.threads(), "kind": "port",
-                         "sample": f"each step: index build of the first {n_sample:.3g} backbone bases ({loci} "
-                                   f"loci), scaled to {n_full} loci; CPU restatement (OpenMP) of the reference's "
-                                   f"bitvector SpGEMM path: the reference's Kokkos build cannot be compiled here"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": orc.threads(), "kind": "port", "sample": sample,
+                         "best_s": min(times), "mean_s": value, "per_step_s": [round(t, 3) for t in times]},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -210,132 +219,242 @@ def config_dict(args, n_loci):
             **({"options": list(args.set)} if args.set else {})}
 
 
-def run_spgemm_micro(args, ctx, stream, rank):
-    """range_spgemm and range_spadd alone on random banded matrices: n = 2^24,
-    band half-width 512, Poisson(4) ranges per row of geometric length
-    (mean 32), canonical, fixed seeds.  Device-resident operands; each timed
-    product is bracketed by CUDA events on the library's stream."""
+def flush_l2(buf):
+    """Writes a buffer larger than L2 (evicts what the last launch left)."""
+    buf.add_(1)
+
+
+# ---- secondary workloads ---------------------------------------------------------
+
+def run_query(args, ctx, stream, d_idx, a, want, npairs=1_000_000, steps=20, warmup=3):
+    """Membership queries (dvg_query_batch, k_query) against the resident
+    chromosome-scale index: npairs locus pairs, half within the distance
+    window, the index (0.8 GB) larger than L2, L2 flushed between launches;
+    each launch bracketed by CUDA events.  Answers compared with the oracle's
+    restatement of CRSMatrixBase::operator() (crs_matrix.hpp:1197-1218)."""
+    import numpy as np
     import torch
     from diverg_b200 import gen
+    pairs = gen.query_pairs(a, npairs, 0.5, args.dmin, args.dmax, seed=args.seed + 11)
+    d_pairs = torch.from_numpy(pairs.view(np.int32).reshape(-1)).cuda()
+    d_out = torch.empty(npairs, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            ctx.query_device(d_idx, d_pairs.data_ptr(), npairs, d_out.data_ptr())
+        ms = []
+        for _ in range(steps):
+            flush_l2(flush)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.query_device(d_idx, d_pairs.data_ptr(), npairs, d_out.data_ptr())
+            e1.record(stream)
+            ms.append((e0, e1))
+        stream.synchronize()
+    t = [e0.elapsed_time(e1) / 1e3 for e0, e1 in ms]
+    mean_s = sum(t) / len(t)
+    got = d_out.cpu().numpy()
+    parity = None
+    if want is not None:
+        from oracle import pyoracle as orc
+        parity = bool(np.array_equal(got, orc.query(want, pairs)))
+    # e2e: host pairs in, host answers out through the C ABI (one call)
+    h_pairs = np.ascontiguousarray(pairs)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        host_ans = ctx.query(d_idx, h_pairs)
+    e2e_s = (time.perf_counter() - t0) / 3
+    peak, peak_kind = peaks()
+    ach = QUERY_ALG_BYTES * npairs / mean_s / 1e9
+    return {"metric": "membership queries/s", "value": npairs / mean_s, "unit": "queries/s",
+            "higher_is_better": True, "steps": steps, "warmup": warmup,
+            "config": {"workload": "membership queries against the resident chromosome-scale index",
+                       "pairs": npairs, "in_window_fraction": 0.5, "window": [args.dmin, args.dmax],
+                       "l2": "index larger than L2, L2 flushed between launches"},
+            "kernel_us": mean_s * 1e6, "ns_per_query": mean_s / npairs * 1e9,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_kind": peak_kind, "alg_bytes_per_query": QUERY_ALG_BYTES,
+                         "note": "random rows: every pair touches at least two 32-byte DRAM sectors (rowmap, range)"},
+            "e2e": {"value": npairs / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(h_pairs.nbytes),
+                    "d2h_bytes_per_step": int(npairs), "note": "pageable host buffers, one call"},
+            "answers_in_range": int(got.sum()), "parity": parity,
+            "e2e_answers_equal": bool(np.array_equal(host_ans, got))}
+
+
+def range_ops_count(a, b):
+    """Work of C = A B on the B side: the B ranges of every B row an A range
+    names, summed over A's ranges (numpy on the host)."""
+    import numpy as np
+    s = a.entries[0::2].astype(np.int64)
+    f = a.entries[1::2].astype(np.int64)
+    br = np.asarray(b.rowmap, dtype=np.int64)
+    return int(((br[f + 1] - br[s]) // 2).sum())
+
+
+def run_spgemm_micro(args, ctx, stream, rank, steps=None, warmup=None):
+    """range_spgemm and range_spadd alone on random banded matrices: n = 2^24,
+    band half-width 512, Poisson(4) ranges per row of geometric length
+    (mean 32), canonical, fixed seeds.  Device-resident operands, L2 flushed
+    between products; each kernel bracketed by CUDA events on the library's
+    stream.  Algorithmic bytes are A + B + C of the product (+ nothing for the
+    union levels the row kernel builds first: their time is counted, their
+    bytes are not)."""
+    import torch
+    from diverg_b200 import gen
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     n = 1 << 24
     a = gen.banded(n, 512, 4.0, 32.0, seed=args.seed + 2 * rank)
     b = gen.banded(n, 512, 4.0, 32.0, seed=args.seed + 2 * rank + 1)
+    rops = range_ops_count(a, b)
     da, db = ctx.upload(a), ctx.upload(b)
     peak, peak_kind = peaks()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
     res = {}
-    for name, op in (("range_spgemm", ctx.spgemm), ("range_spadd", ctx.spadd)):
-        for mode in ((2, 1) if name == "range_spgemm" else (0,)):
-            ctx.set_option("spgemm_mode", mode)
-            for _ in range(args.warmup):
-                op(da, db).free()
-            ctx.set_option("timing", 1)
-            ctx.reset_stats()
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            ev0.record(stream)
-            ranges = 0
-            for _ in range(args.steps):
-                c = op(da, db)
-                ranges = c.nentries // 2
-                c.free()
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            ctx.synchronize()
-            st = ctx.stats()
-            ctx.set_option("timing", 0)
-            kernel_ns = (st["spgemm_symbolic_ns"] + st["spgemm_numeric_ns"] + st["scan_ns"] + st["spadd_ns"])
-            alg = st["alg_bytes"]
-            call_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
-            kern_s = kernel_ns / 1e9 / args.steps
-            gbs = alg / args.steps / kern_s / 1e9
-            res[f"{name}" + ("" if name != "range_spgemm" else ("[row]" if mode == 2 else "[tiled]"))] = {
-                "kernel_ms": kern_s * 1e3, "call_ms": call_s * 1e3, "alg_bytes": alg / args.steps,
-                "achieved_gbs": gbs, "frac": gbs / peak, "output_ranges": ranges,
-                "output_ranges_per_s": ranges / kern_s}
+    variants = (("range_spgemm[automatic]", ctx.spgemm, 0), ("range_spgemm[row+levels]", ctx.spgemm, 2),
+                ("range_spadd", ctx.spadd, 0))
+    for name, op, mode in variants:
+        ctx.set_option("spgemm_mode", mode)
+        for _ in range(warmup):
+            op(da, db).free()
+        ctx.set_option("timing", 1)
+        ctx.reset_stats()
+        ranges = 0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush_l2(flush)
+            c = op(da, db)
+            ranges = c.nentries // 2
+            c.free()
+        ctx.synchronize()
+        st = ctx.stats()
+        ctx.set_option("timing", 0)
+        if name == "range_spadd":
+            kern_ns, lv_ns, alg = st["spadd_ns"] + st["scan_ns"], 0, st["alg_bytes"]
+        else:
+            kern_ns, lv_ns, alg = st["spgemm_ns"], st["spgemm_levels_ns"], st["spgemm_alg_bytes"]
+        kern_s = (kern_ns + lv_ns) / 1e9 / steps
+        gbs = alg / steps / kern_s / 1e9
+        res[name] = {"kernel_ms": kern_s * 1e3, "product_ms": kern_ns / 1e6 / steps, "levels_ms": lv_ns / 1e6 / steps,
+                     "alg_bytes": alg / steps, "achieved_gbs": gbs, "frac": gbs / peak, "output_ranges": ranges,
+                     "output_ranges_per_s": ranges / kern_s}
+        if name != "range_spadd":
+            res[name]["range_ops"] = rops
+            res[name]["range_ops_per_s"] = rops / kern_s
     ctx.set_option("spgemm_mode", 0)
     da.free()
     db.free()
-    best = max((v for k, v in res.items() if k.startswith("range_spgemm")), key=lambda v: v["achieved_gbs"])
+    best = res["range_spgemm[automatic]"]
     return {"metric": "range_spgemm HBM GB/s", "value": best["achieved_gbs"], "unit": "GB/s",
-            "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "higher_is_better": True, "dtype": "u32", "data": "synthetic", "steps": steps, "warmup": warmup,
             "config": {"workload": "kernel microbenchmark: range_spgemm and range_spadd of two random banded "
                                    "matrices", "n": n, "half_width": 512, "ranges_per_row": "Poisson(4)",
                        "range_length": "geometric, mean 32", "seeds": [args.seed, args.seed + 1],
-                       "l2": "operands (0.7 GB each) larger than L2"},
-            "peak": peak, "peak_kind": peak_kind, "kernels": res}
+                       "l2": "operands (0.7 GB each) larger than L2, L2 flushed between products"},
+            "peak": peak, "peak_kind": peak_kind, "kernels": res,
+            "note": "value: the automatic kernel choice (tile-staged here); range_ops = B ranges named by A's "
+                    "ranges, the product's on-chip work"}
 
 
-def cfg3_batch(args, rank):
-    """2,000 graphs of the small-graph generator (bubbles 1/100: 70 % SNP,
+def cfg3_batch(args, rank, ngraphs):
+    """ngraphs graphs of the small-graph generator (bubbles 1/100: 70 % SNP,
     30 % indel of length 1..10), sizes log-normal (median 2e4, sigma 1.0)
     clipped to [1e3, 1e6] bases, windows drawn from {[100,300], [200,500],
     [400,600]}, graph k seeded seed + k."""
     import numpy as np
     from diverg_b200 import gen
     rng = np.random.default_rng(args.seed + 1000 * rank)
-    sizes = np.clip(rng.lognormal(np.log(2e4), 1.0, args.graphs), 1e3, 1e6).astype(np.int64)
+    sizes = np.clip(rng.lognormal(np.log(2e4), 1.0, ngraphs), 1e3, 1e6).astype(np.int64)
     wins = [(100, 300), (200, 500), (400, 600)]
-    windows = [wins[int(i)] for i in rng.integers(0, 3, args.graphs)]
+    windows = [wins[int(i)] for i in rng.integers(0, 3, ngraphs)]
     graphs = [gen.graph_adjacency(gen.small_graph_spec(int(n), seed=args.seed + 1000 * rank + k))[0]
               for k, n in enumerate(sizes)]
     return graphs, windows
 
 
-def run_batch(args, ctx, stream, rank):
+def run_batch(args, ctx, stream, rank, steps=None, warmup=None, oracle_every=20):
+    """Batched builds (dvg_batch_distance_index) against back-to-back plain
+    builds of the same graphs.  Every graph's batched index is compared entry
+    by entry with its plain build, and every oracle_every-th graph with the
+    oracle's CPU build."""
     import numpy as np
     import torch
-    graphs, windows = cfg3_batch(args, rank)
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
+    graphs, windows = cfg3_batch(args, rank, args.graphs)
     dg = [ctx.upload(g) for g in graphs]
     loci = sum(g.numRows() for g in graphs)
     # plain: back-to-back single builds, each bracketed by events
     for k in range(min(50, len(dg))):
         ctx.distance_index(dg[k], *windows[k]).free()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in dg]
-    sizes_plain = []
+    plain = []
     torch.cuda.synchronize()
     for k, (d, w) in enumerate(zip(dg, windows)):
         evs[k][0].record(stream)
         ix = ctx.distance_index(d, *w)
         evs[k][1].record(stream)
-        sizes_plain.append((ix.nentries, ix.nnz))
-        ix.free()
+        plain.append(ix)
     torch.cuda.synchronize()
     lat_plain = np.array([e0.elapsed_time(e1) for e0, e1 in evs])
     plain_s = evs[0][0].elapsed_time(evs[-1][1]) / 1e3
+    plain_host = [ix.download() for ix in plain]
+    for ix in plain:
+        ix.free()
     # batched: warm-up (the first batch autotunes), then timed batches
     ctx.reset_stats()
-    for _ in range(args.warmup):
-        for ix in ctx.batch_distance_index(dg, windows):
-            ix.free()
+    outs = None
+    for i in range(warmup):
+        outs = ctx.batch_distance_index(dg, windows)
+        if i < warmup - 1:
+            for o in outs:
+                o.free()
     tuned = ctx.stats()["autotune_builds"]
+    # parity of the last warm-up batch: every graph against its plain build,
+    # every oracle_every-th against the oracle
+    same_plain = True
+    oracle_checked, oracle_same = 0, True
+    from oracle import pyoracle as orc
+    for k, o in enumerate(outs):
+        h = o.download()
+        p = plain_host[k]
+        same_plain &= (np.array_equal(h.rowmap, p.rowmap) and np.array_equal(h.entries, p.entries)
+                       and h.nnz() == p.nnz())
+        if k % oracle_every == 0:
+            want = orc.dindex(omat(graphs[k]), *windows[k], algo="hbv")
+            oracle_same &= (np.array_equal(h.rowmap, want.rowmap) and np.array_equal(h.entries, want.entries)
+                            and h.nnz() == want.nnz)
+            oracle_checked += 1
+        o.free()
+    del plain_host
     ctx.reset_stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
-    same = True
-    for _ in range(args.steps):
+    for _ in range(steps):
         outs = ctx.batch_distance_index(dg, windows)
-        same = same and all((o.nentries, o.nnz) == sp for o, sp in zip(outs, sizes_plain))
         for o in outs:
             o.free()
     ev1.record(stream)
     torch.cuda.synchronize()
     st = ctx.stats()
-    batch_s = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    batch_s = ev0.elapsed_time(ev1) / 1e3 / steps
     for d in dg:
         d.free()
     n = len(dg)
     return {"metric": "batched index builds/s", "value": n / batch_s, "unit": "builds/s", "higher_is_better": True,
-            "dtype": "u32", "data": "synthetic",
+            "dtype": "u32", "data": "synthetic", "steps": steps, "warmup": warmup,
             "config": {"workload": "batched index builds of mixed-size graphs", "graphs": n, "loci": int(loci),
                        "sizes": "log-normal, median 2e4 bases, sigma 1.0, clipped [1e3, 1e6]",
                        "windows": "uniform over [100,300], [200,500], [400,600]", "seed": args.seed},
             "plain_builds_per_s": n / plain_s, "speedup_vs_plain": plain_s / batch_s,
             "latency_ms": {"batch": batch_s * 1e3, "plain_p50": float(np.percentile(lat_plain, 50)),
                            "plain_p99": float(np.percentile(lat_plain, 99)), "plain_total": plain_s * 1e3},
-            "graph_launches_per_batch": st["graph_launches"] / args.steps,
-            "kernel_launches_per_batch": st["kernel_launches"] / args.steps,
-            "autotune_builds": tuned, "sizes_match_plain": bool(same)}
+            "graph_launches_per_batch": st["graph_launches"] / steps,
+            "kernel_launches_per_batch": st["kernel_launches"] / steps,
+            "autotune_builds": tuned, "parity": {"all_equal_plain": bool(same_plain),
+                                                 "oracle_checked": oracle_checked,
+                                                 "oracle_equal": bool(oracle_same)}}
 
 
 def run_adjacency(args, ctx, stream, rank):
@@ -412,6 +531,26 @@ def apply_options(ctx, pairs):
         ctx.set_option(key.strip(), int(value))
 
 
+def secondary(args, ctx, stream, local, d_idx, a, want):
+    """The secondary workloads after the headline (N = 1), each with its own
+    clock samples and its own step counts (stated in its entry)."""
+    from diverg_b200 import serving
+    out = {}
+    jobs = [("query", lambda: run_query(args, ctx, stream, d_idx, a, want)),
+            ("spgemm", lambda: run_spgemm_micro(args, ctx, stream, 0, steps=5, warmup=3)),
+            ("batch", lambda: run_batch(args, ctx, stream, 0, steps=5, warmup=3)),
+            ("serve", lambda: serving.bench_line(args, ctx, 0, requests=600))]
+    for name, job in jobs:
+        try:
+            with ClockSampler([local]) as clocks:
+                r = job()
+            r["clocks"] = clocks.summary()
+        except Exception as e:  # a secondary failure must not hide the headline
+            r = {"error": f"{type(e).__name__}: {e}"}
+        out[name] = r
+    return out
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -455,13 +594,13 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     d_a = ctx.upload(a)
 
-    idx = None
-    for _ in range(args.warmup):
-        idx = ctx.distance_index(d_a, args.dmin, args.dmax)
-        if _ < args.warmup - 1:
-            idx.free()
-    idx_rows, idx_entries, idx_nnz = idx.nrows, idx.nentries, idx.nnz
-    idx.free()
+    # warm-up; the last warm-up index stays resident (parity, queries)
+    d_idx = None
+    for i in range(args.warmup):
+        d_idx = ctx.distance_index(d_a, args.dmin, args.dmax)
+        if i < args.warmup - 1:
+            d_idx.free()
+    idx_rows, idx_entries, idx_nnz = d_idx.nrows, d_idx.nentries, d_idx.nnz
 
     # ---- timed: device-resident input -------------------------------------
     ctx.reset_stats()
@@ -518,10 +657,11 @@ def main():
         barrier()
         e2e_s = max_over_ranks(e0.elapsed_time(e1)) / 1e3 / args.steps
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        del h_rowmap, h_entries, o_rowmap, o_entries
 
     # ---- roofline of the range-SpGEMM kernel ------------------------------
     peak, peak_kind = peaks()
-    spgemm_ns = st["spgemm_symbolic_ns"] + st["spgemm_numeric_ns"]
+    spgemm_ns = st["spgemm_ns"]
     spgemm_calls = max(1, st["spgemm_calls"])
     per_product_bytes = st["spgemm_alg_bytes"] / spgemm_calls
     per_product_s = spgemm_ns / 1e9 / spgemm_calls
@@ -535,9 +675,29 @@ def main():
                 "kernel": "k_spgemm_rowmode (single-pass range SpGEMM: counts, chunk look-back, runs)",
                 "alg_bytes_per_product": per_product_bytes, "products_per_build": st["spgemm_calls"] / args.steps}
 
-    cpu = None
+    # ---- CPU baseline on the whole graph; its index is the parity oracle ---
+    cpu, want, parity, parity_detail = None, None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, n_loci)
+        t_cpu, want = cpu_build(a, args.dmin, args.dmax)
+        from oracle import pyoracle as orc
+        cpu = {"value": t_cpu, "unit": "s", "cores": orc.threads(), "kind": "port",
+               "sample": f"one index build [{args.dmin},{args.dmax}] of the whole graph ({n_loci} loci), no "
+                         f"scaling; " + cpu_kind_note()}
+        got = d_idx.download()
+        same_rowmap = bool(np.array_equal(got.rowmap.astype(np.uint64), want.rowmap))
+        same_entries = bool(np.array_equal(got.entries, want.entries))
+        same_nnz = got.nnz() == int(want.nnz)
+        parity = same_rowmap and same_entries and same_nnz
+        parity_detail = {"oracle": "the CPU baseline's index (reference schedule, bitvector SpGEMM)",
+                         "gpu_build": "the last warm-up build", "rowmap_equal": same_rowmap,
+                         "entries_equal": same_entries, "nnz_equal": same_nnz,
+                         "rows": int(got.numRows()), "entries": int(got.entries.size), "nnz": int(got.nnz())}
+        del got
+
+    sec = None
+    if world == 1 and not args.no_secondary:
+        sec = secondary(args, ctx, stream, local, d_idx, a, want)
+    del want
 
     if rank == 0:
         steps = args.steps
@@ -550,14 +710,16 @@ def main():
             "gpu_launches": launches,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "parity": parity,
+            "parity_detail": parity_detail,
             "clocks": clocks.summary(),
             "build": {"index_rows": idx_rows, "index_ranges": idx_entries // 2, "index_nnz": idx_nnz,
                       "graph": gstats, "spgemm_per_build": st["spgemm_calls"] / steps,
                       "alg_gb_per_build": st["alg_bytes"] / steps / 1e9,
                       "build_gbs": st["alg_bytes"] / steps / 1e9 / sec_per_build,
                       "kernel_ms_per_build": {
-                          "spgemm_symbolic": st["spgemm_symbolic_ns"] / 1e6 / steps,
-                          "spgemm_numeric": st["spgemm_numeric_ns"] / 1e6 / steps,
+                          "spgemm": st["spgemm_ns"] / 1e6 / steps,
+                          "spgemm_levels": st["spgemm_levels_ns"] / 1e6 / steps,
                           "scan": st["scan_ns"] / 1e6 / steps, "spadd": st["spadd_ns"] / 1e6 / steps},
                       "host_syncs_per_build": st["host_syncs"] / steps,
                       # host side of the timed builds: where the GPU could idle
@@ -566,11 +728,12 @@ def main():
                           "prepare": st_timed["host_prepare_ns"] / 1e6 / steps,
                           "meminfo": st_timed["host_meminfo_ns"] / 1e6 / steps,
                           "launch": st_timed["host_launch_ns"] / 1e6 / steps,
-                          "sync_wait": st_timed["host_sync_ns"] / 1e6 / steps},
-                      "range_ops_per_build": st["range_ops"] / steps},
+                          "sync_wait": st_timed["host_sync_ns"] / 1e6 / steps}},
+            "secondary": sec,
         }
         print(json.dumps(line), flush=True)
 
+    d_idx.free()
     d_a.free()
     ctx.close()
     if world > 1:
@@ -579,7 +742,8 @@ def main():
 
 
 def run_other(args, rank, world, local):
-    """The secondary workloads: one replica per rank, rank 0 prints its line."""
+    """The secondary workloads on their own: one replica per rank, rank 0
+    prints its line."""
     import torch
     import torch.distributed as dist
     from datetime import timedelta
@@ -598,10 +762,21 @@ def run_other(args, rank, world, local):
             line = run_batch(args, ctx, stream, rank)
         elif args.workload == "adjacency":
             line = run_adjacency(args, ctx, stream, rank)
+        elif args.workload == "query":
+            a, _ = graph(args.n_backbone, args.seed + rank)
+            d_a = ctx.upload(a)
+            d_idx = ctx.distance_index(d_a, args.dmin, args.dmax)
+            want = None
+            if not args.no_cpu_baseline:
+                _, want = cpu_build(a, args.dmin, args.dmax)
+            line = run_query(args, ctx, stream, d_idx, a, want, steps=args.steps, warmup=args.warmup)
+            d_idx.free()
+            d_a.free()
         else:
             from diverg_b200 import serving
             line = serving.bench_line(args, ctx, rank)
-    line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "clocks": clocks.summary(),
+    line.update({"n_gpus": world, "steps": line.get("steps", args.steps),
+                 "warmup": line.get("warmup", args.warmup), "clocks": clocks.summary(),
                  "scaling": "weak", "vs_baseline": None})
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -27,7 +27,7 @@ class DvgError(RuntimeError):
 class DvgStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "kernel_launches", "spgemm_calls", "spadd_calls", "host_syncs", "alg_bytes",
-        "spgemm_alg_bytes", "range_ops", "h2d_bytes", "d2h_bytes", "spgemm_symbolic_ns", "spgemm_numeric_ns",
+        "spgemm_alg_bytes", "range_ops", "h2d_bytes", "d2h_bytes", "spgemm_ns", "spgemm_levels_ns",
         "scan_ns", "spadd_ns", "spgemm_direct_tiles", "spgemm_reruns", "spgemm_light", "spgemm_slow_rows", "host_alloc_ns",
         "host_sync_ns", "spgemm_fused_adds", "graph_launches", "autotune_builds", "spgemm_levels",
         "host_prepare_ns", "host_launch_ns", "host_meminfo_ns")]

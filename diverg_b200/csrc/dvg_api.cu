@@ -211,8 +211,8 @@ void resolve_spans(dvg_context* ctx) {
     DVG_CUDA(cudaEventElapsedTime(&ms, t.begin, t.end));
     uint64_t ns = uint64_t(double(ms) * 1e6);
     switch (t.kind) {
-      case kSymbolic: ctx->stats.spgemm_symbolic_ns += ns; break;
-      case kNumeric: ctx->stats.spgemm_numeric_ns += ns; break;
+      case kProduct: ctx->stats.spgemm_ns += ns; break;
+      case kLevels: ctx->stats.spgemm_levels_ns += ns; break;
       case kScan: ctx->stats.scan_ns += ns; break;
       default: ctx->stats.spadd_ns += ns; break;
     }
@@ -267,7 +267,7 @@ static std::vector<dvg_matrix*> build_levels(dvg_context* ctx, const dvg_matrix*
       reset_control(ctx);
       cudaEvent_t t0 = span_begin(ctx);
       launch_row_shifted_sum(ctx, prev, 1u << (k - 1), c->rowmap, c->entries, cap);
-      span_end(ctx, t0, kSymbolic);
+      span_end(ctx, t0, kLevels);
       const DeviceControl ctl = read_control(ctx);
       if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "union levels: chunk look-back wait expired");
       if (ctl.overflow) throw Error(DVG_ERR_DEVICE, "union levels: capacity overflow");
@@ -318,7 +318,7 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
       reset_control(ctx);
       cudaEvent_t t0 = span_begin(ctx);
       launch_spgemm_fused(ctx, a, a_identity, b, d, c->rowmap, c->entries, cap, levels.empty() ? nullptr : &levels);
-      span_end(ctx, t0, kSymbolic);
+      span_end(ctx, t0, kProduct);
       ctl = read_control(ctx);
       if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "range_spgemm: tile look-back wait expired");
       if (!ctl.overflow) break;
@@ -353,7 +353,7 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
 // the same canonical matrix.
 static dvg_matrix* range_spgemm_add(dvg_context* ctx, const dvg_matrix* d, const dvg_matrix* a, const dvg_matrix* b) {
   require(a->ncols == b->nrows && d->nrows == a->nrows && d->ncols == b->ncols, "range_spgemm_add: shapes");
-  if (ctx->opt_algo == 0 && ctx->opt_spgemm_mode != 1) return range_spgemm_fused(ctx, a, false, b, d);
+  if (ctx->opt_spgemm_mode != 1) return range_spgemm_fused(ctx, a, false, b, d);
   dvg_matrix* t = range_spgemm(ctx, a, false, b);
   try {
     dvg_matrix* c = range_spadd(ctx, d, t, false);
@@ -367,41 +367,7 @@ static dvg_matrix* range_spgemm_add(dvg_context* ctx, const dvg_matrix* d, const
 
 dvg_matrix* range_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b) {
   if (!a_identity) require(a->ncols == b->nrows, "range_spgemm: a.numCols() != b.numRows()");
-  if (ctx->opt_algo == 0) return range_spgemm_fused(ctx, a, a_identity, b);
-  const uint32_t n = a_identity ? b->nrows : a->nrows;
-  dvg_matrix* c = new_matrix(ctx, n, b->ncols, 0);
-  try {
-    DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
-    reset_control(ctx);
-    SpgemmPlan plan = plan_spgemm(ctx, a, a_identity, b);
-    cudaEvent_t t0 = span_begin(ctx);
-    launch_spgemm(ctx, plan, a, a_identity, b, c->rowmap, nullptr, false);
-    span_end(ctx, t0, kSymbolic);
-    t0 = span_begin(ctx);
-    launch_rowmap_scan(ctx, c->rowmap, n);
-    span_end(ctx, t0, kScan);
-    uint64_t total = 0;
-    DeviceControl ctl = read_total(ctx, c->rowmap + n, &total);
-    if (total > 0) {
-      dfree(ctx, c->entries);
-      c->entries = nullptr;
-      c->entries = static_cast<uint32_t*>(dalloc(ctx, entries_alloc_bytes(total)));
-      c->nentries = total;
-      t0 = span_begin(ctx);
-      launch_spgemm(ctx, plan, a, a_identity, b, c->rowmap, c->entries, true);
-      span_end(ctx, t0, kNumeric);
-    }
-    c->nnz = ctl.nnz;
-    ctx->stats.spgemm_calls++;
-    uint64_t bytes = (a_identity ? 0 : matrix_bytes(a)) + matrix_bytes(b) + matrix_bytes(c);
-    ctx->stats.alg_bytes += bytes;
-    ctx->stats.spgemm_alg_bytes += bytes;
-    ctx->stats.range_ops += ctl.range_ops;
-  } catch (...) {
-    free_matrix(ctx, c);
-    throw;
-  }
-  return c;
+  return range_spgemm_fused(ctx, a, a_identity, b);
 }
 
 dvg_matrix* range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity) {
@@ -629,7 +595,7 @@ dvg_matrix* create_distance_index(dvg_context* ctx, const dvg_matrix* a, unsigne
   // canonical only for canonical inputs, while the reference's squarings
   // canonicalise any input
   if (ctx->opt_dindex_schedule == 1 || (dlo == 0 && !a->canonical)) return distance_index_reference(ctx, a, dlo, dup);
-  if (ctx->opt_planned && ctx->opt_algo == 0 && ctx->opt_spgemm_mode != 1 && a->nrows > 0) {
+  if (ctx->opt_planned && ctx->opt_spgemm_mode != 1 && a->nrows > 0) {
     PlannedBuild pb;
     bool planned = true;
     try {
@@ -762,16 +728,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
   return guarded([&] {
     Lock lk(ctx);
     require(key != nullptr, "null option key");
-    if (!std::strcmp(key, "group_lanes")) {
-      require(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
-              "group_lanes must be 0, 4, 8, 16 or 32");
-      ctx->opt_group_lanes = value;
-    } else if (!std::strcmp(key, "window_words")) {
-      require(value >= 0 && value <= 4096, "window_words must be in [0, 4096]");
-      ctx->opt_window_words = value;
-    } else if (!std::strcmp(key, "algo")) {
-      require(value == 0 || value == 1, "algo must be 0 (fused tiled) or 1 (two-pass direct)");
-      ctx->opt_algo = value;
+    if (!std::strcmp(key, "algo")) {
+      // the single-pass kernels are the only SpGEMM; 0 is accepted for callers that set it
+      require(value == 0, "algo must be 0 (single-pass SpGEMM)");
     } else if (!std::strcmp(key, "dindex_schedule")) {
       require(value == 0 || value == 1, "dindex_schedule must be 0 (sum of powers) or 1 (reference squaring)");
       ctx->opt_dindex_schedule = value;
@@ -830,20 +789,28 @@ dvg_status dvg_stats_reset(dvg_context* ctx) {
   return DVG_OK;
 }
 
+}  // extern "C"
+
+namespace dvg {
+std::string validation_message(unsigned long long bits) {
+  std::string why;
+  if (bits & 1) why += " rowmap[0] != 0;";
+  if (bits & 2) why += " rowmap decreasing or odd row length;";
+  if (bits & 4) why += " rowmap[nrows] != number of entries;";
+  if (bits & 8) why += " column index >= ncols;";
+  return why;
+}
+}  // namespace dvg
+
+extern "C" {
+
 static void validate_uploaded(dvg_context* ctx, dvg_matrix* m) {
   reset_control(ctx);
   launch_validate(ctx, m->rowmap, m->nrows, m->entries, m->nentries, m->ncols);
   DeviceControl c = read_control(ctx);
   m->canonical = !(c.invalid & 16);
   c.invalid &= ~16ull;
-  if (c.invalid) {
-    std::string why;
-    if (c.invalid & 1) why += " rowmap[0] != 0;";
-    if (c.invalid & 2) why += " rowmap decreasing or odd row length;";
-    if (c.invalid & 4) why += " rowmap[nrows] != number of entries;";
-    if (c.invalid & 8) why += " column index >= ncols;";
-    throw Error(DVG_ERR_INVALID_ARG, "malformed range-CRS matrix:" + why);
-  }
+  if (c.invalid) throw Error(DVG_ERR_INVALID_ARG, "malformed range-CRS matrix:" + validation_message(c.invalid));
 }
 
 static uint64_t count_nnz_host(const uint32_t* e, uint64_t n) {

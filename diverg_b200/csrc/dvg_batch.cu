@@ -200,7 +200,7 @@ void batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dvg_matrix* 
     require(a != nullptr, "batch: null graph");
     require(a->nrows == a->ncols, "batch: adjacency matrix is not square");
     require(dmin[k] <= dmax[k] && dmax[k] != 0, "batch: requires dmin <= dmax and dmax != 0");
-    if ((dmin[k] == 0 && !a->canonical) || !ctx->opt_planned || ctx->opt_algo != 0 || ctx->opt_spgemm_mode == 1 ||
+    if ((dmin[k] == 0 && !a->canonical) || !ctx->opt_planned || ctx->opt_spgemm_mode == 1 ||
         ctx->opt_dindex_schedule != 0)
       alone.push_back(k);
     else

@@ -250,7 +250,7 @@ void launch_build(dvg_context* ctx, PlannedBuild& pb, bool timed) {
     L.slot_variant = pb.slot_variant;
     cudaEvent_t t0 = timed ? span_begin(ctx) : nullptr;
     launch_rowmode(ctx, L, pb.shape);
-    if (t0) span_end(ctx, t0, kSymbolic);
+    if (t0) span_end(ctx, t0, kProduct);
   }
 }
 

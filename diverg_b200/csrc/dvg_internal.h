@@ -63,9 +63,6 @@ struct dvg_context {
   uint32_t* d_pairs = nullptr;        // staging for host-buffer queries
   uint8_t* d_answers = nullptr;
   uint64_t pairs_cap = 0;
-  int64_t opt_group_lanes = 0;
-  int64_t opt_window_words = 0;
-  int64_t opt_algo = 0;               // 0: fused tiled SpGEMM, 1: two-pass direct
   int64_t opt_chunk_rows = 0;         // fused SpGEMM look-back chunk rows (0: automatic)
   int64_t opt_spgemm_mode = 0;        // fused SpGEMM: 0 automatic, 1 tiled, 2 light
   int64_t opt_dindex_schedule = 0;    // 0: sum of powers, 1: the reference's squaring
@@ -131,9 +128,14 @@ void free_matrix(dvg_context* ctx, dvg_matrix* m);
 
 // Kernel timing with CUDA events on ctx->stream (active with the "timing"
 // option): span_begin records a start event, span_end its end and the kind.
-enum TimedKind { kSymbolic = 0, kNumeric = 1, kScan = 2, kSpadd = 3 };
+// kProduct: a single-pass SpGEMM kernel; kLevels: building union levels of B
+enum TimedKind { kProduct = 0, kLevels = 1, kScan = 2, kSpadd = 3 };
 cudaEvent_t span_begin(dvg_context* ctx);
 void span_end(dvg_context* ctx, cudaEvent_t begin, TimedKind kind);
+
+// The failed checks of a validation word (bits 1, 2, 4, 8 of the validation
+// kernels), as "; "-separated text.
+std::string validation_message(unsigned long long bits);
 
 // Reads the control block back (synchronises the stream).
 DeviceControl read_control(dvg_context* ctx);
@@ -152,18 +154,6 @@ void launch_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bo
 // Out-of-range pairs are counted into ctl->invalid (ctx->d_ctl when null).
 void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out,
                   DeviceControl* ctl = nullptr);
-
-struct SpgemmPlan {
-  int group_lanes;   // lanes per output row: 4, 8, 16 or 32
-  int window_words;  // 32-bit accumulator words per group
-};
-SpgemmPlan plan_spgemm(dvg_context* ctx, const dvg_matrix* a, bool a_identity, const dvg_matrix* b);
-// Symbolic (fill = false: c_rowmap[r+1] = entries of row r, nnz and range_ops
-// accumulate in the control block) or numeric (fill = true: rows written at
-// c_rowmap offsets) pass of C = A*B.  a_identity: A is the identity of order
-// b->nrows and `a` is ignored.
-void launch_spgemm(dvg_context* ctx, const SpgemmPlan& plan, const dvg_matrix* a, bool a_identity,
-                   const dvg_matrix* b, uint64_t* c_rowmap, uint32_t* c_entries, bool fill);
 
 // Fused single-pass SpGEMM (dvg_spgemm_fused.cu): writes c_rowmap fully and
 // c_entries up to `cap` entries; the control block receives the total entry

@@ -753,20 +753,15 @@ constexpr uint32_t kNoAllocMaxChunks = 32768;
 constexpr size_t kNoAllocDescBytes = size_t(kNoAllocMaxChunks) * sizeof(ChunkDesc);
 constexpr size_t kNoAllocCtlOffset = kNoAllocDescBytes;                 // DeviceControl
 constexpr size_t kNoAllocTicketOffset = kNoAllocCtlOffset + 256;       // tile ticket
-constexpr size_t kNoAllocBytes = kNoAllocTicketOffset + 256;
+constexpr size_t kNoAllocCheckOffset = kNoAllocTicketOffset + 256;     // validation words of A and B
+constexpr size_t kNoAllocBytes = kNoAllocCheckOffset + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of g_noalloc_scratch per device ordinal.  In host code the
-// array's name is only a host-side stand-in, so the address is looked up once
-// per device (with that device current) and cached here.
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Sets bit 1 of *bad when a range-CRS matrix violates the memory-safety
-// preconditions of the fused kernel (rowmap[0] = 0, non-decreasing, even row
-// lengths, rowmap[n] = nentries, columns < ncols).
+// Records in *bad the memory-safety preconditions of the fused kernel that a
+// range-CRS matrix violates, with the bits of the upload check (1: rowmap[0]
+// != 0, 2: a decreasing rowmap or an odd row length, 4: rowmap[n] !=
+// nentries, 8: a column >= ncols).
 __global__ void k_noalloc_validate(const uint64_t* __restrict__ rowmap, uint32_t nrows,
                                    const uint32_t* __restrict__ entries, uint64_t nentries, uint32_t ncols,
                                    unsigned long long* bad) {
@@ -775,12 +770,15 @@ __global__ void k_noalloc_validate(const uint64_t* __restrict__ rowmap, uint32_t
   const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
   for (uint64_t i = tid; i < nrows; i += stride) {
     const uint64_t lo = rowmap[i], hi = rowmap[i + 1];
-    if (hi < lo || ((hi - lo) & 1)) b = 1;
+    if (hi < lo || ((hi - lo) & 1)) b |= 2;
   }
-  if (tid == 0 && (rowmap[0] != 0 || rowmap[nrows] != nentries)) b = 1;
+  if (tid == 0) {
+    if (rowmap[0] != 0) b |= 1;
+    if (rowmap[nrows] != nentries) b |= 4;
+  }
   for (uint64_t i = tid; i < nentries; i += stride)
-    if (entries[i] >= ncols) b = 1;
-  if (b) atomicOr(bad, 1ull);
+    if (entries[i] >= ncols) b |= 8;
+  if (b) atomicOr(bad, b);
 }
 
 dvg_status dvg_noalloc_fail(dvg_status s, const std::string& msg) {
@@ -819,20 +817,18 @@ extern "C" dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncol
   try {
     int dev = 0;
     DVG_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) throw Error(DVG_ERR_DEVICE, "device ordinal out of range");
-    unsigned char* scratch = nullptr;
-    {
-      std::lock_guard<std::mutex> lk(g_noalloc_mu);
-      if (!g_noalloc_ptr[dev]) {
-        void* ptr = nullptr;
-        DVG_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = ptr;
-      }
-      scratch = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
-    }
+    // In host code g_noalloc_scratch names a host-side stand-in, not device
+    // memory: the array's address on the current device comes from the
+    // runtime.  It is looked up on every call (a host-side table lookup)
+    // rather than kept, because a device reset or a new primary context
+    // reloads the module and may move the array.
+    void* scratch_ptr = nullptr;
+    DVG_CUDA(cudaGetSymbolAddress(&scratch_ptr, g_noalloc_scratch));
+    unsigned char* scratch = static_cast<unsigned char*>(scratch_ptr);
     ChunkDesc* desc = reinterpret_cast<ChunkDesc*>(scratch);
     DeviceControl* ctl = reinterpret_cast<DeviceControl*>(scratch + kNoAllocCtlOffset);
     unsigned* ticket = reinterpret_cast<unsigned*>(scratch + kNoAllocTicketOffset);
+    unsigned long long* check = reinterpret_cast<unsigned long long*>(scratch + kNoAllocCheckOffset);
     DeviceControl h{};
     if (a_nrows == 0) {
       DVG_CUDA(cudaMemsetAsync(d_c_rowmap, 0, sizeof(uint64_t), stream));
@@ -842,18 +838,22 @@ extern "C" dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncol
     // 1. inputs must be well formed before the product may index through them
     int nsm = 0;
     DVG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    DVG_CUDA(cudaMemsetAsync(ctl, 0, sizeof(DeviceControl), stream));
+    DVG_CUDA(cudaMemsetAsync(check, 0, 2 * sizeof(unsigned long long), stream));
     const unsigned vgrid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(
         (std::max<uint64_t>(std::max<uint64_t>(a_nrows, a_nentries), std::max<uint64_t>(b_nrows, b_nentries)) +
          255) / 256, uint64_t(nsm) * 8)));
-    k_noalloc_validate<<<vgrid, 256, 0, stream>>>(d_a_rowmap, a_nrows, d_a_entries, a_nentries, a_ncols,
-                                                  &ctl->invalid);
-    k_noalloc_validate<<<vgrid, 256, 0, stream>>>(d_b_rowmap, b_nrows, d_b_entries, b_nentries, b_ncols,
-                                                  &ctl->invalid);
+    k_noalloc_validate<<<vgrid, 256, 0, stream>>>(d_a_rowmap, a_nrows, d_a_entries, a_nentries, a_ncols, check);
+    k_noalloc_validate<<<vgrid, 256, 0, stream>>>(d_b_rowmap, b_nrows, d_b_entries, b_nentries, b_ncols, check + 1);
     DVG_CUDA(cudaGetLastError());
-    DVG_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, stream));
+    unsigned long long bad[2] = {0, 0};
+    DVG_CUDA(cudaMemcpyAsync(bad, check, sizeof(bad), cudaMemcpyDeviceToHost, stream));
     DVG_CUDA(cudaStreamSynchronize(stream));
-    if (h.invalid) throw Error(DVG_ERR_INVALID_ARG, "malformed range-CRS input matrix");
+    if (bad[0] || bad[1]) {
+      std::string why;
+      if (bad[0]) why += " A:" + validation_message(bad[0]);
+      if (bad[1]) why += " B:" + validation_message(bad[1]);
+      throw Error(DVG_ERR_INVALID_ARG, "malformed range-CRS input matrix;" + why);
+    }
     // 2. the fused product with this file's scratch
     auto kern = k_spgemm_fused<false>;
     const int smem = int(sizeof(Smem));
@@ -885,7 +885,7 @@ extern "C" dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncol
     p.chunk_rows = chunk_rows;
     p.nchunks = nchunks;
     p.row_mode = 0;
-      const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
+    const unsigned grid = unsigned(std::min<uint64_t>(nchunks, resident));
     kern<<<grid, kThreads, smem, stream>>>(p);
     DVG_CUDA(cudaGetLastError());
     DVG_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost, stream));

@@ -185,13 +185,17 @@ def run_stream(server, graphs, pair_pool, answer_pool, rate, nreq, seed, window=
             "all_latency_ms": _percentiles(lat[BUILD] + lat[QUERY]), "builds": [b for b, _ in built]}
 
 
-def bench_line(args, ctx, rank):
+def bench_line(args, ctx, rank, requests=None, max_rate=51200.0):
     """The serving benchmark: graphs of 1e4..1e6 bases (log-uniform) from the
     small-graph generator, window [200, 500], query batches of 1e5..1e6 pairs
-    (half within the window), HBM budget 150 GB, Poisson arrivals swept over
-    rates; the knee is the highest rate still served at >= 95 % of it."""
+    (half within the window), HBM budget 150 GB, Poisson arrivals.  Without a
+    fixed rate the sweep doubles the arrival rate from 200/s until the served
+    throughput falls below 95 % of the offered rate (or a request fails): the
+    knee is the highest rate still served at >= 95 % of it, and the first
+    rate past it is reported beside it."""
     import torch
     from . import gen
+    nreq = int(requests or args.requests)
     rng = np.random.default_rng(args.seed + 7 * rank)
     ngraphs = 48
     sizes = np.exp(rng.uniform(np.log(1e4), np.log(1e6), ngraphs)).astype(np.int64)
@@ -202,16 +206,27 @@ def bench_line(args, ctx, rank):
         p = gen.query_pairs(g, 1_000_000, 0.5, 200, 500, seed=args.seed + k)
         pair_pool.append(torch.from_numpy(p.view(np.int32)).pin_memory())
     answer_pool = [torch.empty(1_000_000, dtype=torch.uint8).pin_memory() for _ in range(64)]
-    rates = [args.rate] if args.rate > 0 else [100.0, 200.0, 400.0, 800.0, 1600.0]
     sweep = []
+    saturated = None
     with Server(device=ctx.device, hbm_budget_bytes=150 * 10**9, max_inflight_queries=8) as srv:
         warm = [srv.submit_build(g, 200, 500) for g in graphs[:8]]
         srv.wait(warm)
-        for i, rate in enumerate(rates):
-            r = run_stream(srv, graphs, pair_pool, answer_pool, rate, args.requests, args.seed + 100 + i)
+        rate, i = (args.rate if args.rate > 0 else 200.0), 0
+        while True:
+            r = run_stream(srv, graphs, pair_pool, answer_pool, rate, nreq, args.seed + 100 + i)
             for b in r.pop("builds"):
                 srv.release(b)
             sweep.append(r)
+            ok = r["throughput"] >= 0.95 * r["rate"] and r["failed"] == 0
+            if args.rate > 0:
+                break
+            if not ok:
+                saturated = r
+                break
+            if rate * 2 > max_rate:
+                break
+            rate *= 2
+            i += 1
         st = srv.stats()
     served = [r for r in sweep if r["throughput"] >= 0.95 * r["rate"] and r["failed"] == 0]
     knee = max(served, key=lambda r: r["rate"]) if served else min(sweep, key=lambda r: r["rate"])
@@ -219,9 +234,13 @@ def bench_line(args, ctx, rank):
             "higher_is_better": True, "dtype": "u32", "data": "synthetic",
             "config": {"workload": "serving loop over a mixed Poisson-arrival stream", "builds": "20 %, graphs of "
                        "1e4..1e6 bases (log-uniform), window [200,500]", "queries": "80 %, batches of 1e5..1e6 "
-                       "pairs, half within the window", "hbm_budget_gb": 150, "requests_per_rate": args.requests,
+                       "pairs, half within the window", "hbm_budget_gb": 150, "requests_per_rate": nreq,
                        "seed": args.seed},
             "knee_rate": knee["rate"], "latency_ms_at_knee": {"build": knee["build_latency_ms"],
                                                               "query": knee["query_latency_ms"],
                                                               "all": knee["all_latency_ms"]},
+            "saturated_at": None if saturated is None else {"rate": saturated["rate"],
+                                                            "throughput": saturated["throughput"],
+                                                            "failed": saturated["failed"]},
+            "knee_measured": saturated is not None,
             "sweep": sweep, "server": st}

@@ -57,8 +57,8 @@ typedef struct dvg_stats {
   uint64_t d2h_bytes;
   /* device time of the kernels, measured with CUDA events on the context's
    * stream while the "timing" option is on (0 otherwise) */
-  uint64_t spgemm_symbolic_ns;  /* SpGEMM symbolic passes */
-  uint64_t spgemm_numeric_ns;   /* SpGEMM numeric passes */
+  uint64_t spgemm_ns;           /* single-pass SpGEMM kernels (counts, offsets and runs in one pass) */
+  uint64_t spgemm_levels_ns;    /* building union levels of B for long-range products */
   uint64_t scan_ns;             /* rowmap scans (SpGEMM and SpAdd) */
   uint64_t spadd_ns;            /* SpAdd passes */
   uint64_t spgemm_direct_tiles; /* SpGEMM row tiles that missed the staged path */
@@ -89,10 +89,7 @@ dvg_status dvg_shutdown(dvg_context* ctx);
  * context's own stream). */
 dvg_status dvg_set_stream(dvg_context* ctx, void* cuda_stream);
 dvg_status dvg_synchronize(dvg_context* ctx);
-/* Tuning knobs: "algo" (0 = fused single-pass tile-staged SpGEMM, the
- * default; 1 = two-pass row-direct SpGEMM), "group_lanes" (two-pass path: 0 =
- * autotune, or 4/8/16/32 lanes per output row), "window_words" (two-pass path:
- * 0 = default, else 32-bit accumulator words per row group), "chunk_rows"
+/* Tuning knobs: "algo" (0 only: the single-pass SpGEMM kernels), "chunk_rows"
  * (fused path: 0 = automatic, else rows per output chunk, a multiple of 32 up
  * to 2048), "spgemm_mode" (fused path: 0 = automatic -- tile-staged when A's
  * ranges average more than 8 columns, else a thread per row --, 1 =
@@ -226,15 +223,23 @@ dvg_status dvg_adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uin
  * Its scratch is a fixed array inside the library (about 1 MiB, held on every
  * GPU that loads the library until the process exits), which limits the
  * product to a_nrows <= 67,108,864; larger products are rejected with
- * DVG_ERR_INVALID_ARG.  The first call on a device looks up that array's
- * device address; make this first call before any stream capture.  All calls
- * share the array: calls whose work overlaps on the GPU race and must be
- * serialised by the caller.
+ * DVG_ERR_INVALID_ARG.  Every call looks up that array's device address on
+ * the current device.  All calls share the array: calls whose work overlaps
+ * on the GPU race and must be serialised by the caller.
+ *
+ * The inputs are checked on the device before the product reads through
+ * them; a malformed A or B (rowmap[0] != 0, a decreasing rowmap or odd row
+ * length, rowmap[n] != nentries, a column >= ncols) returns
+ * DVG_ERR_INVALID_ARG, names the operand and the checks in dvg_last_error(),
+ * and leaves d_c_rowmap untouched.  The product always runs the tile-staged
+ * kernel; dvg_range_spgemm picks the thread-per-row kernel for short-range
+ * operands and is faster there.
  *
  * d_c_rowmap holds a_nrows + 1 entries; d_c_entries holds c_capacity entries.
  * On return *c_nentries and *c_nnz describe C.  If c_capacity is too small
  * the call returns DVG_ERR_OVERFLOW with c_rowmap complete and *c_nentries
- * set to the required capacity.  The call synchronises `cuda_stream`. */
+ * set to the required capacity.  The call waits on `cuda_stream` twice: once
+ * for the input checks and once for the product's size. */
 dvg_status dvg_range_spgemm_noalloc(uint32_t a_nrows, uint32_t a_ncols, const uint64_t* d_a_rowmap,
                                     const uint32_t* d_a_entries, uint64_t a_nentries, uint32_t b_nrows,
                                     uint32_t b_ncols, const uint64_t* d_b_rowmap, const uint32_t* d_b_entries,

@@ -1,8 +1,9 @@
 """Generates the committed golden fixtures under tests/golden/.
 
-Run here (where the reference checkout exists), never on the GPU host:
+Run where a checkout of the reference exists, never on the GPU host; the
+checkout's path is a required argument:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 It reads the reference's own test data as text:
   * the HBitVector known-answer vectors of test/src/test_hbitvector.cpp
@@ -27,7 +28,9 @@ sys.path.insert(0, os.path.join(HERE, "..", ".."))
 
 from oracle import pyoracle as orc  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+    sys.exit("usage: python tests/golden/make_golden.py /path/to/reference-checkout")
+REF = sys.argv[1]
 
 
 # ---- known-answer vectors -----------------------------------------------------

@@ -10,13 +10,10 @@ from tests.conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-# (algo, group lanes, window words[, fused mode]): the fused kernel in its
-# automatic (thread per row), tile-staged and thread-per-row modes, then the two-pass
-# row-direct kernel at "auto", every group size at its default window, and
-# tiny windows that force its multi-chunk path
+# (algo, group lanes, window words, SpGEMM mode): the single-pass kernels in
+# their automatic choice, the tile-staged rows and the thread-per-row mode
 FUSED = [(0, 0, 0, 0), (0, 0, 0, 1), (0, 0, 0, 2)]
-PLANS = FUSED + [(1, 0, 0), (1, 4, 0), (1, 8, 0), (1, 16, 0), (1, 32, 0), (1, 4, 1), (1, 8, 3), (1, 32, 2),
-                 (1, 16, 37)]
+PLANS = FUSED
 
 
 @pytest.fixture(scope="module")
@@ -27,9 +24,6 @@ def ctx():
 
 
 def set_plan(ctx, plan, chunk_rows=0):
-    ctx.set_option("algo", plan[0])
-    ctx.set_option("group_lanes", plan[1])
-    ctx.set_option("window_words", plan[2])
     ctx.set_option("spgemm_mode", plan[3] if len(plan) > 3 else 0)
     ctx.set_option("chunk_rows", chunk_rows)
 
@@ -61,7 +55,7 @@ def test_hbitvector_known_answer(ctx, plan):
 
 
 @pytest.mark.parametrize("name", ["x", "multi", "m"])
-@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0), (1, 4, 0), (1, 32, 0), (1, 8, 3)])
+@pytest.mark.parametrize("plan", FUSED)
 def test_gfa_fixture_products(ctx, name, plan):
     set_plan(ctx, plan)
     g = load_golden(f"gfa_{name}.npz")
@@ -91,7 +85,7 @@ def test_random_spgemm_reference_shape(ctx, plan):
     assert_same(ctx.spgemm(da, da).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0), (1, 4, 0), (1, 16, 0), (1, 8, 5)])
+@pytest.mark.parametrize("plan", FUSED)
 def test_random_power_reference_shape(ctx, plan):
     # test_range_sparse.cpp:590-594: N = 6521, NNZ = 4000, K = 100
     set_plan(ctx, plan)
@@ -109,7 +103,7 @@ def test_random_spadd_reference_shapes(ctx, n, nnz):
     assert_same(ctx.spadd(ctx.upload(a), ctx.upload(b)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0)])
+@pytest.mark.parametrize("plan", FUSED)
 def test_rectangular_spgemm(ctx, plan):
     set_plan(ctx, plan)
     a = gen.random_matrix(3000, 30000, seed=5)
@@ -120,7 +114,7 @@ def test_rectangular_spgemm(ctx, plan):
         assert_same(ctx.spgemm(ctx.upload(x), ctx.upload(y)).download(), want.rowmap, want.entries, want.nnz)
 
 
-@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0), (1, 8, 0), (1, 32, 4)])
+@pytest.mark.parametrize("plan", FUSED)
 def test_banded_spgemm(ctx, plan):
     set_plan(ctx, plan)
     a = gen.banded(1 << 16, 512, 4.0, 32.0, seed=31)
@@ -144,7 +138,7 @@ def test_small_graph_index(ctx, window, plan, chunk_rows, schedule):
     assert_same(got, want.rowmap, want.entries, want.nnz, str(window))
 
 
-@pytest.mark.parametrize("plan", FUSED + [(1, 0, 0)])
+@pytest.mark.parametrize("plan", FUSED)
 @pytest.mark.parametrize("schedule", [0, 1])
 def test_graph_with_structural_bubbles_index(ctx, plan, schedule):
     set_plan(ctx, plan)
@@ -221,7 +215,7 @@ def test_algos_agree_on_cfg2_shape_sample(ctx):
     a = gen.banded(1 << 20, 512, 4.0, 32.0, seed=51)
     b = gen.banded(1 << 20, 512, 4.0, 32.0, seed=52)
     want = orc.spgemm(omat(a), omat(b), algo="hbv")
-    for plan in FUSED + [(1, 0, 0)]:
+    for plan in FUSED:
         set_plan(ctx, plan)
         got = ctx.spgemm(ctx.upload(a), ctx.upload(b)).download()
         assert_same(got, want.rowmap, want.entries, want.nnz, f"plan {plan}")

@@ -5,9 +5,10 @@ a latency-critical path that cannot afford cudaMalloc's synchronisation).
 
 The test calls it through the C ABI with caller-owned device buffers and
 checks its output, exactly (integer data), against the allocating entry point
-dvg_range_spgemm on two different products in a row -- the second call runs on
-the scratch the first one left behind.  It also checks the capacity overflow
-contract and the size limit.  This file is collected last on purpose.
+dvg_range_spgemm and the CPU oracle on two different products in a row -- the
+second call runs on the scratch the first one left behind.  It also checks the
+capacity overflow contract, the size limit and the rejection of malformed
+inputs on the device.  This file is collected last on purpose.
 """
 import ctypes
 
@@ -16,6 +17,7 @@ import pytest
 
 from diverg_b200 import _native as N, gen
 from diverg_b200.runtime import Context
+from oracle import pyoracle as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -58,6 +60,11 @@ def test_noalloc_matches_the_allocating_spgemm_on_two_calls_in_a_row():
             got_entries = c_entries[:ne].cpu().numpy().view(np.uint32)
             assert np.array_equal(got_rowmap, want.rowmap)
             assert np.array_equal(got_entries, want.entries)
+            ha, hb = a.download(), b.download()
+            ref = orc.spgemm(orc.OMat(ha.numRows(), ha.numCols(), ha.rowmap.astype(np.uint64), ha.entries, ha.nnz()),
+                             orc.OMat(hb.numRows(), hb.numCols(), hb.rowmap.astype(np.uint64), hb.entries, hb.nnz()))
+            assert np.array_equal(got_rowmap, ref.rowmap) and np.array_equal(got_entries, ref.entries)
+            assert nz == ref.nnz
     finally:
         ctx.close()
 
@@ -89,3 +96,46 @@ def test_noalloc_rejects_products_beyond_its_scratch():
                                           dummy, 0, ctypes.byref(ne), ctypes.byref(nz), ctypes.c_void_p(0))
     assert st == N.INVALID_ARG
     assert b"67108864" in N.lib().dvg_last_error()
+
+
+# (rowmap, entries, ncols, nentries passed, the check the message names): small
+# matrices that break one precondition each; every read of the check stays
+# inside the buffers (rowmap[0..n], entries[0..nentries))
+MALFORMED = [
+    ([2, 2, 4], [0, 1, 2, 3], 8, 4, "rowmap[0] != 0"),
+    ([0, 3, 4], [0, 1, 2, 3], 8, 4, "odd row length"),
+    ([0, 2, 4], [0, 1, 2, 3], 8, 2, "rowmap[nrows] != number of entries"),
+    ([0, 2, 4], [0, 1, 2, 8], 8, 4, "column index >= ncols"),
+]
+
+
+@pytest.mark.parametrize("case", MALFORMED, ids=[c[4] for c in MALFORMED])
+@pytest.mark.parametrize("operand", ["A", "B"])
+def test_noalloc_rejects_malformed_inputs_before_the_product(case, operand):
+    import torch
+    rowmap, entries, ncols, nent, why = case
+    bad_r = torch.tensor(np.array(rowmap, dtype=np.uint64).view(np.int64), device="cuda")
+    bad_e = torch.tensor(np.array(entries, dtype=np.uint32).view(np.int32), device="cuda")
+    n = len(rowmap) - 1
+    # a well-formed n x ncols (as A) or ncols x ncols (as B) partner: the identity
+    good_n = ncols if operand == "A" else n
+    good_r = torch.tensor(np.arange(0, 2 * good_n + 1, 2, dtype=np.uint64).view(np.int64), device="cuda")
+    good_e = torch.tensor(np.repeat(np.arange(good_n, dtype=np.uint32), 2).view(np.int32), device="cuda")
+    if operand == "A":
+        a = (n, ncols, bad_r, bad_e, nent)
+        b = (ncols, ncols, good_r, good_e, 2 * ncols)
+    else:
+        a = (n, n, good_r, good_e, 2 * n)
+        b = (n, ncols, bad_r, bad_e, nent)
+    c_rowmap = torch.full((a[0] + 1,), -1, dtype=torch.int64, device="cuda")
+    c_entries = torch.full((64,), -1, dtype=torch.int32, device="cuda")
+    ne, nz = ctypes.c_uint64(), ctypes.c_uint64()
+    st = N.lib().dvg_range_spgemm_noalloc(
+        a[0], a[1], ctypes.c_void_p(a[2].data_ptr()), ctypes.c_void_p(a[3].data_ptr()), a[4],
+        b[0], b[1], ctypes.c_void_p(b[2].data_ptr()), ctypes.c_void_p(b[3].data_ptr()), b[4],
+        ctypes.c_void_p(c_rowmap.data_ptr()), ctypes.c_void_p(c_entries.data_ptr()), c_entries.numel(),
+        ctypes.byref(ne), ctypes.byref(nz), ctypes.c_void_p(0))
+    msg = N.lib().dvg_last_error().decode()
+    assert st == N.INVALID_ARG, msg
+    assert f"{operand}:" in msg and why in msg, msg
+    assert bool((c_rowmap == -1).all()) and bool((c_entries == -1).all())
