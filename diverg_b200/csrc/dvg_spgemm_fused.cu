@@ -101,12 +101,7 @@ __device__ __forceinline__ uint32_t row_mask(const BBuf& B, uint64_t b_base, uin
   return m;
 }
 
-// 8-byte asynchronous global -> shared copy (completes at cp.async.wait_group).
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
-  const uint32_t d = uint32_t(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// (cp_async8 and cp_async_commit: dvg_spgemm_common.cuh)
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned runtime_group_mask(int g) {

@@ -72,122 +72,6 @@ struct RowSmem {
   uint32_t nslow;
 };
 
-// CTA barrier that counts threads, not warps: the non-aligned form of
-// barrier.sync, which the lanes of a warp may reach at different times.  The
-// row loop leaves the lanes of a warp on paths of very different length (one
-// lane walks a wide row while the others wait), and the aligned form
-// (__syncthreads) is only defined for warps that arrive converged.  Every
-// barrier of the row kernel is this one, on barrier 0.
-__device__ __forceinline__ void cta_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
-
-// Asynchronous 8-byte copy global -> shared (cp.async): the copy lands while
-// the thread goes on; cp_async_wait() waits for all of the thread's copies.
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const uint32_t sa = uint32_t(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// A descriptor word (flag | value) for other CTAs' look-backs.  The word is
-// all a reader takes from it -- no other data of the writer is read on its
-// strength -- so a relaxed store does: a release would first wait for every
-// earlier store of the thread (its share of a chunk image) to land.
-__device__ __forceinline__ void st_relaxed(unsigned long long* q, unsigned long long v) {
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(q), "l"(v) : "memory");
-}
-
-// Publishes chunk t's aggregate (its entries) for later chunks' look-backs.
-__device__ __forceinline__ void publish_aggregate(const FusedArgs& p, uint32_t t, unsigned long long cnt) {
-  st_relaxed(&p.desc[t].agg, kFlag | cnt);
-}
-
-// The whole CTA walks back from chunk t (whose aggregate is published),
-// kThreads descriptors a round, summing aggregates down to the nearest
-// inclusive prefix; every thread gets t's exclusive prefix and thread 0
-// publishes t's inclusive prefix (and, for the last chunk, the total).  A
-// deferred chunk's predecessors have mostly published aggregates but not yet
-// prefixes, so the walk is a few hundred descriptors deep: one round here.
-// A round is one 16-byte load per thread and one barrier: each warp reduces
-// its 32 descriptors (newest first) to a record -- the sum up to its first
-// prefix, whether it has one, whether a descriptor before that has nothing
-// yet -- and every thread scans the 16 records in order.  The records
-// alternate between two sets by round (`par` runs on across calls), so a
-// round's writes never meet the previous round's reads.  Waits are bounded;
-// every branch is uniform over the CTA.
-template <int SLOT>
-__device__ unsigned long long lookback_block(RowSmem<SLOT>& S, const FusedArgs& p, uint32_t t,
-                                             unsigned long long cnt, uint32_t& par) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  ChunkDesc* d = p.desc;
-  unsigned long long pre = 0;
-  int64_t j = int64_t(t) - 1;
-  uint32_t spins = 0;
-  while (j >= 0) {
-    const int64_t idx = j - tid;
-    int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: nothing yet
-    unsigned long long v = 0;
-    if (idx >= 0) {
-      unsigned long long va, vi;
-      asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(va), "=l"(vi) : "l"(&d[idx].agg) : "memory");
-      if (vi & kFlag) {
-        v = vi & ~kFlag;
-      } else if (va & kFlag) {
-        st = 1;
-        v = va & ~kFlag;
-      } else {
-        st = 0;
-      }
-    }
-    const unsigned im = __ballot_sync(kFullMask, st == 2), wm = __ballot_sync(kFullMask, st == 0);
-    const int fi = im ? __ffs(im) - 1 : 32;
-    const unsigned before = fi == 32 ? kFullMask : ((1u << fi) - 1u);
-    unsigned long long sv = lane <= fi ? v : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(kFullMask, sv, o);
-    if (lane == 0) {
-      S.lb_sum[par][warp] = sv;
-      S.lb_flag[par][warp] = (fi < 32 ? 1u : 0u) | ((wm & before) ? 2u : 0u);
-    }
-    cta_sync();
-    unsigned long long tot = 0;
-    bool done = false, wait = false;
-#pragma unroll 1
-    for (int w = 0; w < kWarps; ++w) {
-      const uint32_t f = S.lb_flag[par][w];
-      if (f & 2u) {
-        wait = true;
-        break;
-      }
-      tot += S.lb_sum[par][w];
-      if (f & 1u) {
-        done = true;
-        break;
-      }
-    }
-    par ^= 1u;
-    if (wait) {  // a chunk after the nearest prefix has published nothing yet
-      if (++spins > (p.spin_limit ? p.spin_limit : kSpinLimit)) {
-        if (tid == 0) raise_flag(p, &p.ctl->timeout, 1ull);
-        break;
-      }
-      __nanosleep(64);
-      continue;
-    }
-    pre += tot;
-    if (done) break;
-    j -= kThreads;
-  }
-  if (tid == 0) {
-    st_relaxed(&d[t].incl, kFlag | (pre + cnt));
-    if (t == p.nchunks - 1) {
-      p.ctl->total = pre + cnt;
-      if (pre + cnt > p.cap) raise_flag(p, &p.ctl->overflow, pre + cnt);
-    }
-  }
-  return pre;
-}
-
 // Accumulates chunk row r (C row `row`) into the thread's slot from entry
 // `pos` on.  A's row pointers come from the stage, its ranges from the stage
 // when they are among the chunk's first kAStage ranges (abase: the chunk's
@@ -709,6 +593,7 @@ RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_
   }
   RowLaunchShape s{};
   s.resident = ctx->row_resident[v];
+  if (ctx->opt_row_window) s.resident = std::min(s.resident, window_resident(ctx));
   // chunk rows: as large as possible (fewer look-back steps) while keeping
   // about four chunks per resident CTA
   uint32_t chunk_rows = kChunkMax;
@@ -747,6 +632,14 @@ void selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit) {
 
 void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& s) {
   if (L.nrows == 0) return;
+  // the window kernel stages with 8-byte asynchronous copies
+  const uintptr_t mis = reinterpret_cast<uintptr_t>(L.a_rowmap) | reinterpret_cast<uintptr_t>(L.a_entries) |
+                        reinterpret_cast<uintptr_t>(L.b_rowmap) | reinterpret_cast<uintptr_t>(L.b_entries) |
+                        reinterpret_cast<uintptr_t>(L.d_rowmap) | reinterpret_cast<uintptr_t>(L.d_entries);
+  if (ctx->opt_row_window && L.nlevels == 0 && (mis & 7u) == 0) {
+    launch_rowmode_window(ctx, L, s);
+    return;
+  }
   const int v = std::min(std::max(L.slot_variant, 0), 2);
   FusedArgs p{};
   p.a_rowmap = L.a_identity ? nullptr : L.a_rowmap;
