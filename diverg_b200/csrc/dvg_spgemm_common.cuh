@@ -24,6 +24,7 @@ constexpr int kBitWords = 6144;   // union bitmaps (PRE, SUF, BU) or direct wind
 constexpr int kStageMax = 6144;   // output entries staged per chunk
 constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
 constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
+constexpr int kRowScratchPerRow = 8;  // window kernel: scratch entries a chunk row (rows of several runs)
 constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
 constexpr int kMaxLevels = 12;    // union levels of B (blocks of up to 4096 rows)
 constexpr unsigned long long kFlag = 1ull << 63;

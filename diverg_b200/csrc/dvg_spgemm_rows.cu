@@ -66,8 +66,12 @@ struct RowSmem {
   unsigned long long lb_sum[2][kWarps];  // look-back records by round parity, per warp
   uint32_t lb_flag[2][kWarps];
   uint32_t phase[kWarps];               // iterations per warp, checked at every iteration's end
-  unsigned long long pend_cnt;          // the staged chunk waiting in buffer b ^ 1
-  uint32_t pend_t, pend_crows;
+  // the staged chunk waiting in image buffer k, kept per buffer: its readers
+  // (the next iteration) and the writer of the next one (that iteration's
+  // end, which a look-back of no rounds may not separate from them by a
+  // barrier) never meet on one slot
+  unsigned long long pend_cnt[2];
+  uint32_t pend_t[2], pend_crows[2];
   uint32_t next;                        // the chunk taken for the next iteration
   uint32_t nslow;
 };
@@ -421,8 +425,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     }
     // the pending chunk: look-back, row map, one coalesced copy
     if (pend) {
-      const uint32_t pend_t = S.pend_t, pend_crows = S.pend_crows;
-      const unsigned long long pend_cnt = S.pend_cnt;
+      const uint32_t pend_t = S.pend_t[b ^ 1u], pend_crows = S.pend_crows[b ^ 1u];
+      const unsigned long long pend_cnt = S.pend_cnt[b ^ 1u];
       const unsigned long long prefix = lookback_block(S, p, pend_t, pend_cnt, par);
       const uint32_t* img = stage + size_t(b ^ 1u) * (p.stage_cap + p.chunk_rows);
       const uint32_t* pincl = img + p.stage_cap;
@@ -531,6 +535,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         }
       }
     }
+    if (tid == 0 && staged) {  // the image just written, in buffer b
+      S.pend_t[b] = t;
+      S.pend_crows[b] = crows;
+      S.pend_cnt[b] = cnt;
+    }
     if (staged) {
       pend = true;
       b ^= 1u;
@@ -538,14 +547,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     // the next chunk; every warp must have passed the same barriers
     ++iter;
     if (lane == 0) S.phase[warp] = iter;
-    if (tid == 0) {
-      if (staged) {
-        S.pend_t = t;
-        S.pend_crows = crows;
-        S.pend_cnt = cnt;
-      }
-      S.nslow = 0;
-    }
+    if (tid == 0) S.nslow = 0;
     cta_sync();
     if (warp == 0) {  // one read per lane, one vote
       const bool off = lane < kWarps && S.phase[lane] != iter;
@@ -603,7 +605,8 @@ RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_
   s.nchunks = uint32_t((uint64_t(nrows) + chunk_rows - 1) / chunk_rows);
   s.grid = uint32_t(std::min<uint64_t>(s.nchunks, s.resident));
   s.desc_bytes = size_t(s.nchunks) * sizeof(ChunkDesc);
-  s.stage_bytes = size_t(s.grid) * 2 * (kRowStagePerRow + 1) * s.chunk_rows * sizeof(uint32_t);
+  // per CTA two image buffers, then (the window kernel) a scratch for rows of several runs
+  s.stage_bytes = size_t(s.grid) * (2 * (kRowStagePerRow + 1) + kRowScratchPerRow) * s.chunk_rows * sizeof(uint32_t);
   return s;
 }
 
@@ -636,7 +639,7 @@ void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& 
   const uintptr_t mis = reinterpret_cast<uintptr_t>(L.a_rowmap) | reinterpret_cast<uintptr_t>(L.a_entries) |
                         reinterpret_cast<uintptr_t>(L.b_rowmap) | reinterpret_cast<uintptr_t>(L.b_entries) |
                         reinterpret_cast<uintptr_t>(L.d_rowmap) | reinterpret_cast<uintptr_t>(L.d_entries);
-  if (ctx->opt_row_window && L.nlevels == 0 && (mis & 7u) == 0) {
+  if (ctx->opt_row_window && L.nlevels == 0 && L.stage_buf && (mis & 7u) == 0) {
     launch_rowmode_window(ctx, L, s);
     return;
   }

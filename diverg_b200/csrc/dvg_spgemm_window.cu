@@ -25,14 +25,16 @@
 // outside a staged window, or a chunk whose ranges exceed a stage's capacity,
 // falls back to reading HBM for the missing part; results are identical.
 //
-// Rows are walked twice from shared memory: once to count (runs, nnz), once,
-// after the chunk's prefix, to emit the runs into the chunk's image -- the
-// operands are on chip, so recomputing is cheaper than keeping every row's
-// runs (the other kernel's run-list slots).  A row's closed runs sit in a
-// 4-run list in shared memory while it is walked; rows with more runs take
-// the warp-cooperative path.  Output order, deferred write-out through per-CTA
-// staging buffers, the CTA-wide decoupled look-back, bounded waits, the abort
-// word of planned builds and every self-check are those of k_spgemm_rowmode.
+// Each row is walked once, from shared memory.  A row of one run keeps it in
+// shared memory (frun), a row of more runs writes them to a per-CTA scratch
+// in global memory (L2-resident, 8 entries a row); rows whose runs overflow
+// the walk's 4-run list are recomputed from HBM by the warp-cooperative path.
+// So once a chunk is counted its stages are dead, and the next chunk's
+// operands are requested at once: their latency overlaps the counted chunk's
+// prefix and image and the write-out of the chunk before it.  Output order,
+// deferred write-out through per-CTA staging buffers, the CTA-wide decoupled
+// look-back, bounded waits, the abort word of planned builds and every
+// self-check are those of k_spgemm_rowmode.
 #include <algorithm>
 
 #include "dvg_spgemm_common.cuh"
@@ -42,31 +44,39 @@ namespace {
 
 constexpr int kWRows = kChunkMax;          // rows per chunk (upper bound)
 constexpr int kWRpt = kWRows / kThreads;   // rows per thread at the largest chunk
-constexpr int kWAEnt = 2048;               // A ranges staged per chunk
-constexpr int kWDEnt = 2048;               // addend ranges staged per chunk
+// stage capacities: a little above a chunk's rows, as index products average
+// slightly more than one range a row (a chunk that holds more reads the rest
+// from HBM)
+constexpr int kWAEnt = 2304;               // A ranges staged per chunk
+constexpr int kWDEnt = 2304;               // addend ranges staged per chunk
 constexpr int kWBRows = 2559;              // B rows in the staged window (at most)
-constexpr int kWBEnt = 2560;               // B ranges staged per chunk
-constexpr int kWList = 8;                  // run-list entries per thread (four closed runs)
-constexpr int kWDirectWarps = 4;           // warps that run the warp path
+constexpr int kWBEnt = 2688;               // B ranges staged per chunk
+constexpr int kWList = 8;                  // run-list entries per walking thread (four closed runs)
+constexpr int kWGenThreads = 256;          // threads that walk the general rows
+constexpr int kWRowScratch = kRowScratchPerRow;  // scratch entries a row (four runs)
+constexpr int kWDirectWarps = 2;           // warps that run the warp path
 constexpr int kWDirectWW = 192;            // warp path: 32-bit window words per warp
 constexpr int kWRowStagePerRow = 16;       // image entries per chunk row, as the staging buffers are sized
 
-// Shared memory of one CTA.  The two 64-bit row-pointer runs of the next
-// chunk land in `bent` + `list` (adjacent) before they are compacted to
-// 32 bits, and the B window's row pointers land in `bent` before the B
+// Shared memory of one CTA.  The next chunk's 64-bit A row pointers land in
+// `bent` and its addend row pointers in `dent` before they are compacted to
+// 16 bits, and the B window's row pointers land in `bent` before the B
 // ranges do: those arrays are free while a chunk is being staged.
 struct WinSmem {
   uint2 aent[kWAEnt];     // the chunk's A ranges (from abase on)
   uint2 dent[kWDEnt];     // the chunk's addend ranges (from dbase on)
   uint2 bent[kWBEnt];     // the B window's ranges (from bbase on)
-  uint32_t list[kWList * kThreads];  // closed runs of the row in hand: entry k of thread t at [k * kThreads + t]
-  // low 32 bits of range offsets (rowmap / 2): A and addend rows c0 .. c0 + crows,
-  // B rows wlo .. whi + 1; row r spans [x[r] - x[0], x[r + 1] - x[0]) of its stage
-  uint32_t arow[kWRows + 1];
-  uint32_t drow[kWRows + 1];
-  uint32_t brow[kWBRows + 1];
+  uint2 frun[kWRows];     // the counted chunk's rows: the run of a one-run row, or a kFrun* marker
+  uint32_t list[kWList * kWGenThreads];  // closed runs of the row in hand: entry k of thread t at [k * kWGenThreads + t]
+  // low 16 bits of range offsets (rowmap / 2): A and addend rows c0 .. c0 + crows,
+  // B rows wlo .. wlo + wn; row r spans [rel(x, r), rel(x, r + 1)) of its stage
+  // (16-bit differences: a chunk's rows are used only while it holds < 2^16 ranges)
+  uint16_t arow[kWRows + 1];
+  uint16_t drow[kWRows + 1];
+  uint16_t brow[kWBRows + 1];
   uint32_t incl[kWRows];      // the counted chunk's (then chunk-local inclusive) row counts
   uint32_t slow[kSlowMax];    // rows of the counted chunk left to the warp path
+  uint16_t gen[kWRows];       // rows of the counted chunk left to the general walk (kinds marked)
   uint32_t direct[2 * kWDirectWW * kWDirectWarps];  // warp path: bits + reach per warp
   unsigned long long red[kWarps];
   unsigned long long red_nnz[kWarps];
@@ -75,20 +85,31 @@ struct WinSmem {
   uint32_t phase[kWarps];                // iterations per warp, checked at every iteration's end
   uint32_t wmin[kWarps], wmax[kWarps];   // per-warp bounds of the chunk's A ranges
   unsigned long long abase, dbase, bbase;  // 64-bit range offset of each stage's first range
-  unsigned long long pend_cnt;           // the staged chunk waiting in buffer b ^ 1
+  // the staged chunk waiting in image buffer k, kept per buffer: its readers
+  // (the next iteration) and the writer of the next one (that iteration's
+  // end, which a look-back of no rounds may not separate from them by a
+  // barrier) never meet on one slot
+  unsigned long long pend_cnt[2];
   uint32_t na, nd, nb;                   // ranges staged
-  uint32_t rows_ok;                      // bit 0: arow usable, bit 1: drow usable
+  uint32_t rows_ok;                      // bit 0: arow usable, bit 1: drow usable (< 2^16 ranges)
   uint32_t wlo, wn;                      // staged B rows [wlo, wlo + wn)
   uint32_t wn_req;                       // B rows whose row pointers were requested (from wlo)
-  uint32_t pend_t, pend_crows;
+  uint32_t pend_t[2], pend_crows[2];
   uint32_t next;                         // the chunk taken for the next iteration
   uint32_t nslow;
+  uint32_t ngen;
 };
 static_assert(sizeof(WinSmem) <= 115712, "two CTAs per SM must fit");
-static_assert(offsetof(WinSmem, list) == offsetof(WinSmem, bent) + sizeof(uint2) * kWBEnt, "bent, list adjacent");
-static_assert(sizeof(uint2) * kWBEnt + sizeof(uint32_t) * kWList * kThreads >= 2 * 8 * (kWRows + 1),
-              "the next chunk's row pointers fit bent + list");
+static_assert(sizeof(uint2) * kWBEnt >= 8 * (kWRows + 1) && sizeof(uint2) * kWDEnt >= 8 * (kWRows + 1),
+              "the next chunk's row pointers fit bent and dent");
 static_assert(sizeof(uint2) * kWBEnt >= 8 * (kWBRows + 1), "the B window's row pointers fit bent");
+
+// frun markers (x > y, so no run): the row's runs are in the CTA's scratch,
+// or are recomputed by the warp path, or by the per-thread bit-window walk.
+constexpr uint32_t kFrunScratch = 0xffffffffu, kFrunWarp = 0xfffffffeu, kFrunLight = 0xfffffffdu;
+
+// Offset of row k's first range from row 0's in a stage of 16-bit words.
+__device__ __forceinline__ uint32_t rel(const uint16_t* x, uint32_t k) { return uint16_t(x[k] - x[0]); }
 
 // ---- staging ------------------------------------------------------------------
 // Four phases, each ended by the next one's wait: (1) request the chunk's A
@@ -100,7 +121,7 @@ static_assert(sizeof(uint2) * kWBEnt >= 8 * (kWBRows + 1), "the B window's row p
 template <bool A_ID>
 __device__ void stage_req_rows(WinSmem& S, const FusedArgs& p, uint32_t c0row, uint32_t crows) {
   uint64_t* rawA = reinterpret_cast<uint64_t*>(S.bent);
-  uint64_t* rawD = rawA + (kWRows + 1);
+  uint64_t* rawD = reinterpret_cast<uint64_t*>(S.dent);
   for (uint32_t k = threadIdx.x; k <= crows; k += kThreads) {
     if (!A_ID) cp_async8(rawA + k, p.a_rowmap + uint64_t(c0row) + k);
     if (p.d_rowmap) cp_async8(rawD + k, p.d_rowmap + uint64_t(c0row) + k);
@@ -111,12 +132,12 @@ __device__ void stage_req_rows(WinSmem& S, const FusedArgs& p, uint32_t c0row, u
 template <bool A_ID>
 __device__ void stage_rows_req_ranges(WinSmem& S, const FusedArgs& p, uint32_t crows) {
   const uint64_t* rawA = reinterpret_cast<const uint64_t*>(S.bent);
-  const uint64_t* rawD = rawA + (kWRows + 1);
+  const uint64_t* rawD = reinterpret_cast<const uint64_t*>(S.dent);
   cp_async_wait();
   cta_sync();
   for (uint32_t k = threadIdx.x; k <= crows; k += kThreads) {
-    if (!A_ID) S.arow[k] = uint32_t(rawA[k] >> 1);
-    if (p.d_rowmap) S.drow[k] = uint32_t(rawD[k] >> 1);
+    if (!A_ID) S.arow[k] = uint16_t(rawA[k] >> 1);
+    if (p.d_rowmap) S.drow[k] = uint16_t(rawD[k] >> 1);
   }
   // every thread reads the same words: the stage sizes are uniform
   uint64_t abase = 0, na64 = 0, dbase = 0, nd64 = 0;
@@ -135,8 +156,8 @@ __device__ void stage_rows_req_ranges(WinSmem& S, const FusedArgs& p, uint32_t c
     S.dbase = dbase;
     S.na = na;
     S.nd = nd;
-    // 32-bit row offsets hold while a chunk's ranges stay below 2^31
-    S.rows_ok = (na64 < (1ull << 31) ? 1u : 0u) | (nd64 < (1ull << 31) ? 2u : 0u);
+    // 16-bit row offsets hold while a chunk's ranges stay below 2^16
+    S.rows_ok = (na64 < (1ull << 16) ? 1u : 0u) | (nd64 < (1ull << 16) ? 2u : 0u);
   }
   cta_sync();  // the raw words are dead from here on
   for (uint32_t k = threadIdx.x; k < na; k += kThreads) cp_async8(&S.aent[k], p.a_entries + 2 * (abase + k));
@@ -217,7 +238,7 @@ __device__ void stage_brows_req_branges(WinSmem& S, const FusedArgs& p) {
     }
     nb64 = (raw[wn] >> 1) - bbase;
   }
-  for (uint32_t k = tid; k <= wn && wn; k += kThreads) S.brow[k] = uint32_t(raw[k] >> 1);
+  for (uint32_t k = tid; k <= wn && wn; k += kThreads) S.brow[k] = uint16_t(raw[k] >> 1);
   if (tid == 0) {
     S.wn = wn;
     S.bbase = bbase;
@@ -242,46 +263,124 @@ __device__ void stage_chunk(WinSmem& S, const FusedArgs& p, uint32_t t) {
 }
 
 // ---- one row ---------------------------------------------------------------------
+//
+// Nearly every row of an index product is the union of at most two ranges:
+// its addend range and the one range of the B row its single A range names
+// (measured on the products of a synthetic chromosome graph: 97-99.8 % of
+// rows).  fast_row does such a row on a short straight path from the stages
+// and returns true, with count = its entries, its nnz accumulated and its
+// runs kept (a run in frun[r]; two runs in the row's scratch slot `scr`);
+// any other row (more ranges, unstaged data, union levels) returns false and
+// is listed for the general walk, which the CTA spreads over kWGenThreads
+// threads -- a handful of general rows per chunk, so no warp waits on a warp
+// that met one.
+template <bool A_ID>
+__device__ __forceinline__ bool fast_row(WinSmem& S, const FusedArgs& p, uint32_t row, uint32_t r, uint32_t& count,
+                                         unsigned long long& nnz, uint32_t* scr) {
+  const uint32_t rows_ok = S.rows_ok;
+  bool fast = p.nlevels == 0;
+  uint2 u = make_uint2(1u, 0u), v = make_uint2(1u, 0u);  // the row's (at most) two input ranges
+  if (p.d_identity) {
+    u = make_uint2(uint32_t(row), uint32_t(row));
+  } else if (p.d_rowmap) {
+    const uint32_t d0 = rel(S.drow, r), d1 = rel(S.drow, r + 1);
+    if (!(rows_ok & 2u) || d1 - d0 > 1u || (d1 > d0 && d0 >= S.nd)) fast = false;
+    else if (d1 > d0) u = S.dent[d0];
+  }
+  uint2 ar;
+  if (A_ID) {
+    ar = id_range(p, row);
+  } else {
+    const uint32_t a0 = rel(S.arow, r), a1 = rel(S.arow, r + 1);
+    if (!(rows_ok & 1u) || a1 - a0 != 1u || a0 >= S.na) {
+      fast = false;
+      ar = make_uint2(1u, 0u);
+    } else {
+      ar = S.aent[a0];
+    }
+  }
+  if (fast && ar.x <= ar.y) {
+    const uint32_t wlo = S.wlo;
+    if (ar.x >= wlo && ar.y - wlo < S.wn) {
+      const uint32_t t0 = rel(S.brow, ar.x - wlo), t1 = rel(S.brow, ar.y + 1 - wlo);
+      if (t1 - t0 > 1u) fast = false;
+      else if (t1 > t0) v = S.bent[t0];
+    } else {
+      fast = false;
+    }
+  }
+  if (!fast) return false;
+  {
+    const bool hu = u.x <= u.y, hv = v.x <= v.y;
+    if (hu && hv && v.x < u.x) {
+      const uint2 w = u;
+      u = v;
+      v = w;
+    }
+    uint32_t nr;
+    uint2 r0 = hu ? u : v, r1 = v;
+    if (hu && hv) {
+      if (v.x <= u.y || v.x - u.y == 1u) {  // overlapping or adjacent: one run
+        r0 = make_uint2(u.x, max(u.y, v.y));
+        nr = 1;
+      } else {
+        nr = 2;
+      }
+    } else {
+      nr = (hu || hv) ? 1u : 0u;
+    }
+    if (nr == 2) {
+      *reinterpret_cast<uint4*>(scr) = make_uint4(r0.x, r0.y, r1.x, r1.y);
+      S.frun[r] = make_uint2(kFrunScratch, 0u);
+    } else {
+      S.frun[r] = r0;
+    }
+    count = 2 * nr;
+    nnz += (nr ? uint64_t(r0.y - r0.x) + 1 : 0) + (nr == 2 ? uint64_t(r1.y - r1.x) + 1 : 0);
+    return true;
+  }
+}
 
-// Walks C row `row` (chunk row r) from the stages (HBM for what is not
-// staged) into the thread's run list.  EMIT = false: count = entries of the
-// row, nnz accumulated; returns false, leaving no trace in nnz, when the runs
-// overflow the list.  EMIT = true: writes the row's `n` entries to out[0..n)
-// and returns false if the row does not have exactly n.
-template <bool A_ID, bool EMIT>
-__device__ bool win_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r, uint32_t& count,
-                        unsigned long long& nnz, uint32_t* out, uint32_t n_out) {
+// The general walk of C row `row` (chunk row r) from the stages (HBM for what
+// is not staged) into the thread's run list (threads < kWGenThreads).
+// Returns true with count = the row's entries, its nnz accumulated and its
+// runs kept as fast_row keeps them (more than one run: in its scratch slot
+// `scr`); false, leaving no trace, when the runs overflow the list.
+template <bool A_ID>
+__device__ bool general_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r, uint32_t& count,
+                            unsigned long long& nnz, uint32_t* scr) {
+  constexpr uint32_t kT = kWGenThreads;
   uint32_t* L = S.list + threadIdx.x;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
   constexpr uint32_t max_runs = kWList / 2;
   uint32_t nr = 0;
   // merges [x, y] into the list; false when it needs more runs than fit
   auto merge = [&](uint32_t x, uint32_t y) -> bool {
     uint32_t k = 0;
-    while (k < nr && uint64_t(L[(2 * k + 1) * kThreads]) + 1 < x) ++k;
-    if (k == nr || uint64_t(y) + 1 < L[2 * k * kThreads]) {
+    while (k < nr && uint64_t(L[(2 * k + 1) * kT]) + 1 < x) ++k;
+    if (k == nr || uint64_t(y) + 1 < L[2 * k * kT]) {
       if (nr == max_runs) return false;
       for (uint32_t m = nr; m > k; --m) {
-        L[2 * m * kThreads] = L[2 * (m - 1) * kThreads];
-        L[(2 * m + 1) * kThreads] = L[(2 * m - 1) * kThreads];
+        L[2 * m * kT] = L[2 * (m - 1) * kT];
+        L[(2 * m + 1) * kT] = L[(2 * m - 1) * kT];
       }
-      L[2 * k * kThreads] = x;
-      L[(2 * k + 1) * kThreads] = y;
+      L[2 * k * kT] = x;
+      L[(2 * k + 1) * kT] = y;
       ++nr;
       return true;
     }
-    uint32_t lo = min(L[2 * k * kThreads], x), hi = max(L[(2 * k + 1) * kThreads], y);
+    uint32_t lo = min(L[2 * k * kT], x), hi = max(L[(2 * k + 1) * kT], y);
     uint32_t m = k + 1;
-    while (m < nr && uint64_t(hi) + 1 >= L[2 * m * kThreads]) {
-      hi = max(hi, L[(2 * m + 1) * kThreads]);
+    while (m < nr && uint64_t(hi) + 1 >= L[2 * m * kT]) {
+      hi = max(hi, L[(2 * m + 1) * kT]);
       ++m;
     }
-    L[2 * k * kThreads] = lo;
-    L[(2 * k + 1) * kThreads] = hi;
+    L[2 * k * kT] = lo;
+    L[(2 * k + 1) * kT] = hi;
     const uint32_t gone = m - k - 1;
     if (gone) {
       for (uint32_t q = m; q < nr; ++q) {
-        L[2 * (q - gone) * kThreads] = L[2 * q * kThreads];
-        L[(2 * (q - gone) + 1) * kThreads] = L[(2 * q + 1) * kThreads];
+        L[2 * (q - gone) * kT] = L[2 * q * kT];
+        L[(2 * (q - gone) + 1) * kT] = L[(2 * q + 1) * kT];
       }
       nr -= gone;
     }
@@ -315,8 +414,8 @@ __device__ bool win_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r
   } else if (p.d_rowmap) {
     uint64_t d0, d1;
     if (rows_ok & 2u) {
-      d0 = S.drow[r] - S.drow[0];
-      d1 = S.drow[r + 1] - S.drow[0];
+      d0 = rel(S.drow, r);
+      d1 = rel(S.drow, r + 1);
     } else {
       d0 = (__ldg(p.d_rowmap + row) >> 1) - S.dbase;
       d1 = (__ldg(p.d_rowmap + row + 1) >> 1) - S.dbase;
@@ -329,8 +428,8 @@ __device__ bool win_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r
   uint64_t a0 = 0, a1 = 1;
   if (!A_ID) {
     if (rows_ok & 1u) {
-      a0 = S.arow[r] - S.arow[0];
-      a1 = S.arow[r + 1] - S.arow[0];
+      a0 = rel(S.arow, r);
+      a1 = rel(S.arow, r + 1);
     } else {
       a0 = (__ldg(p.a_rowmap + row) >> 1) - S.abase;
       a1 = (__ldg(p.a_rowmap + row + 1) >> 1) - S.abase;
@@ -360,7 +459,7 @@ __device__ bool win_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r
     }
     if (ar.x >= wlo && uint64_t(ar.y) < uint64_t(wlo) + wn) {
       // every B range of rows s..f is staged (the window's ranges are whole rows)
-      const uint32_t t0 = S.brow[ar.x - wlo] - S.brow[0], t1 = S.brow[ar.y + 1 - wlo] - S.brow[0];
+      const uint32_t t0 = rel(S.brow, ar.x - wlo), t1 = rel(S.brow, ar.y + 1 - wlo);
       for (uint32_t t = t0; t < t1; ++t)
         if (!take(S.bent[t])) return false;
     } else {
@@ -370,28 +469,37 @@ __device__ bool win_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r
     }
   }
   if (any && !merge(run_lo, run_hi)) return false;
-  if (EMIT) {
-    if (2 * nr != n_out) return false;
-    for (uint32_t k = 0; k < nr; ++k) {
-      out[2 * k] = L[2 * k * kThreads];
-      out[2 * k + 1] = L[(2 * k + 1) * kThreads];
+  uint64_t n = 0;
+  for (uint32_t k = 0; k < nr; ++k) {
+    const uint32_t lo = L[2 * k * kT], hi = L[(2 * k + 1) * kT];
+    n += uint64_t(hi - lo) + 1;
+    if (nr > 1) {
+      scr[2 * k] = lo;
+      scr[2 * k + 1] = hi;
     }
-  } else {
-    uint64_t n = 0;
-    for (uint32_t k = 0; k < nr; ++k) n += uint64_t(L[(2 * k + 1) * kThreads]) - L[2 * k * kThreads] + 1;
-    count = 2 * nr;
-    nnz += n;
   }
+  if (nr == 1) S.frun[r] = make_uint2(L[0], L[kT]);
+  else if (nr > 1) S.frun[r] = make_uint2(kFrunScratch, 0u);
+  count = 2 * nr;
+  nnz += n;
   return true;
 }
 
 // ---- the kernel --------------------------------------------------------------------
 // With rpt = ceil(chunk_rows / kThreads) rows per thread, thread (warp, lane)
 // owns chunk rows (warp * rpt + u) * 32 + lane, u < rpt: the lanes of a warp
-// take consecutive rows.  An iteration counts chunk t (staged), takes its
-// prefix, writes its image to staging buffer b (or, when it does not fit,
-// resolves it in place), and resolves the chunk staged one iteration before
-// while the next chunk's operands are requested.
+// take consecutive rows.  An iteration counts chunk t from its stages, then
+// -- with the stages dead -- requests chunk t+1's operands phase by phase
+// between its remaining steps: the warp path, the chunk's prefix, its image
+// in staging buffer b (or, when it does not fit, its write-out in place) and
+// the write-out of the chunk staged one iteration before (look-back, row
+// map, one coalesced copy).
+//
+// Rows of a chunk: fast rows (fast_row) by their own thread; the rest, listed
+// in S.gen, by the general walk spread over kWGenThreads threads; rows whose
+// runs overflow the general walk's list by the warp path (S.slow, kSlowMax a
+// chunk) or, past that list, by the per-thread bit-window walk (light_row),
+// both recomputing from HBM when the runs are written.
 template <bool A_ID>
 __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -401,52 +509,122 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
   uint32_t* dreach = dbits + kWDirectWW;
   const uint32_t rpt = (p.chunk_rows + kThreads - 1) / kThreads;  // 1..kWRpt
   // per CTA two buffers: a chunk's image (stage_cap entries), then its
-  // chunk-local inclusive row counts (chunk_rows words)
-  uint32_t* const stage =
-      p.stage_buf ? p.stage_buf + size_t(blockIdx.x) * 2 * (p.stage_cap + p.chunk_rows) : nullptr;
+  // chunk-local inclusive row counts (chunk_rows words); after every CTA's
+  // buffers, per CTA kWRowScratch entries a chunk row for rows of several runs
+  uint32_t* const stage = p.stage_buf + size_t(blockIdx.x) * 2 * (p.stage_cap + p.chunk_rows);
+  uint32_t* const scratch = p.stage_buf + size_t(gridDim.x) * 2 * (p.stage_cap + p.chunk_rows) +
+                            size_t(blockIdx.x) * kWRowScratch * p.chunk_rows;
   // a planned build stops at the first step whose output is unusable
-  auto take_ticket = [&]() -> uint32_t {
-    const bool stop = p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
-    return stop ? 0xffffffffu : atomicAdd(p.ticket, 1u);
-  };
+  auto stopped = [&]() { return p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0; };
   if (tid == 0) {
-    S.next = take_ticket();
+    S.next = stopped() ? 0xffffffffu : atomicAdd(p.ticket, 1u);
     S.nslow = 0;
+    S.ngen = 0;
   }
   cta_sync();
   uint32_t t = S.next, b = 0, par = 0;
   bool pend = false;  // a staged chunk waits in buffer b ^ 1 (described in S.pend_*)
   if (t < p.nchunks) stage_chunk<A_ID>(S, p, t);
   uint32_t iter = 0;
+  // writes the runs of every row of the counted chunk at base + its
+  // chunk-local offset (base: the image, or C at the chunk's prefix); a row
+  // past `cap` entries of base is not written (an overflow is raised)
+  auto write_rows = [&](uint32_t c0row, uint32_t crows, uint32_t nslow, uint32_t* base, unsigned long long cap) {
+    const uint32_t* incl = S.incl;
+#pragma unroll 1
+    for (int u = 0; u < kWRpt; ++u) {
+      if (uint32_t(u) >= rpt) break;
+      const uint32_t r = (warp * rpt + u) * 32 + lane;
+      if (r >= crows) continue;
+      const uint32_t o = r ? incl[r - 1] : 0u;
+      const uint32_t n = incl[r] - o;
+      if (n == 0) continue;
+      const uint2 f = S.frun[r];
+      if (f.x == kFrunWarp) continue;  // the warp path below
+      if (uint64_t(o) + n > cap) {     // only a chunk written in place can meet the end of C
+        raise_flag(p, &p.ctl->overflow, 1ull);
+        continue;
+      }
+      uint32_t* out = base + o;
+      if (f.x <= f.y) {
+        if (n != 2) raise_flag(p, &p.ctl->status, 8ull);
+        out[0] = f.x;
+        out[1] = f.y;
+      } else if (f.x == kFrunScratch) {
+        const uint32_t* scr = scratch + size_t(r) * kWRowScratch;
+        if (n > uint32_t(kWRowScratch)) raise_flag(p, &p.ctl->status, 8ull);
+        else
+          for (uint32_t k = 0; k < n; ++k) out[k] = __ldcg(scr + k);
+      } else {
+        const uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
+                                           [&](uint64_t k, uint32_t v) {
+                                             if (k < n) out[k] = v;
+                                           });
+        if (c != n) raise_flag(p, &p.ctl->status, 8ull);
+      }
+    }
+    if (warp < kWDirectWarps) {
+      for (uint32_t i = warp; i < nslow; i += kWDirectWarps) {
+        const uint32_t r = S.slow[i];
+        const uint32_t o = r ? incl[r - 1] : 0u;
+        const uint32_t n = incl[r] - o;
+        if (n == 0) continue;
+        if (uint64_t(o) + n > cap) {
+          if (lane == 0) raise_flag(p, &p.ctl->overflow, 1ull);
+          continue;
+        }
+        uint32_t* out = base + o;
+        bool bad = false;
+        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
+                                      [&](uint64_t k, uint32_t v) {
+                                        if (k < n) out[k] = v;
+                                        else bad = true;
+                                      },
+                                      kWDirectWW);
+        if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+      }
+    }
+  };
   while (t < p.nchunks || pend) {
     const bool have = t < p.nchunks;
     // the stage of chunk t may still be landing (requested last iteration)
     cp_async_wait();
     cta_sync();
-    const bool stop = tid == 0 && p.abort && *reinterpret_cast<volatile unsigned long long*>(p.abort) != 0;
-    uint32_t next = 0xffffffffu;
     const uint32_t c0row = have ? t * p.chunk_rows : 0u;
     const uint32_t crows = have ? min(p.chunk_rows, p.nrows - c0row) : 0u;
     uint32_t* const incl = S.incl;
     unsigned long long nnz_acc = 0, cnt = 0, cnnz = 0;
-    uint32_t fast_mask = 0, nslow = 0, nslow_all = 0;
+    uint32_t nslow = 0;
     bool staged = false;
     if (have) {
-      // count: every row from the stages
+      // the next chunk, taken while this one is counted
+      if (tid == 0) S.next = stopped() ? 0xffffffffu : atomicAdd(p.ticket, 1u);
+      // count: fast rows by their threads, the rest listed
 #pragma unroll 1
       for (int u = 0; u < kWRpt; ++u) {
         if (uint32_t(u) >= rpt) break;
         const uint32_t r = (warp * rpt + u) * 32 + lane;
         if (r < crows) {
           uint32_t c = 0;
-          if (win_row<A_ID, false>(S, p, uint64_t(c0row) + r, r, c, nnz_acc, nullptr, 0)) {
-            fast_mask |= 1u << u;
-          } else {
-            const uint32_t i = atomicAdd(&S.nslow, 1u);
-            if (i < uint32_t(kSlowMax)) {
-              S.slow[i] = r;
+          if (fast_row<A_ID>(S, p, c0row + r, r, c, nnz_acc, scratch + size_t(r) * kWRowScratch)) incl[r] = c;
+          else S.gen[atomicAdd(&S.ngen, 1u)] = uint16_t(r);
+        }
+      }
+      cta_sync();
+      // the general walk, spread over kWGenThreads threads
+      const uint32_t ngen = S.ngen;
+      if (tid < kWGenThreads) {
+        for (uint32_t i = tid; i < ngen; i += kWGenThreads) {
+          const uint32_t r = S.gen[i];
+          uint32_t c = 0;
+          if (!general_row<A_ID>(S, p, uint64_t(c0row) + r, r, c, nnz_acc, scratch + size_t(r) * kWRowScratch)) {
+            const uint32_t j = atomicAdd(&S.nslow, 1u);
+            if (j < uint32_t(kSlowMax)) {
+              S.slow[j] = r;
+              S.frun[r] = make_uint2(kFrunWarp, 0u);
             } else {
               c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
+              S.frun[r] = make_uint2(kFrunLight, 0u);
             }
             atomicAdd(&p.ctl->slow_rows, 1ull);
           }
@@ -454,18 +632,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
         }
       }
       cta_sync();
-      if (tid == 0 && !stop) next = atomicAdd(p.ticket, 1u);
-      nslow_all = S.nslow;
-      nslow = min(nslow_all, uint32_t(kSlowMax));
-      if (warp < kWDirectWarps) {
-        for (uint32_t i = warp; i < nslow; i += kWDirectWarps) {
-          const uint32_t r = S.slow[i];
-          const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
-                                        [](uint64_t, uint32_t) {}, kWDirectWW);
-          if (lane == 0) incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+    }
+    // the counted chunk's stages are dead: request the next chunk's operands
+    const uint32_t tn = S.next;
+    const bool pre = have && tn < p.nchunks;
+    const uint32_t n0row = pre ? tn * p.chunk_rows : 0u;
+    const uint32_t ncrows = pre ? min(p.chunk_rows, p.nrows - n0row) : 0u;
+    if (pre) stage_req_rows<A_ID>(S, p, n0row, ncrows);
+    if (have) {
+      nslow = min(S.nslow, uint32_t(kSlowMax));
+      if (nslow) {
+        if (warp < kWDirectWarps) {
+          for (uint32_t i = warp; i < nslow; i += kWDirectWarps) {
+            const uint32_t r = S.slow[i];
+            const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
+                                          [](uint64_t, uint32_t) {}, kWDirectWW);
+            if (lane == 0) incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+          }
         }
+        cta_sync();
       }
-      cta_sync();
       // chunk prefix over the row counts (kWRpt consecutive rows per thread:
       // a thread rewrites only its own rows) and the chunk's nnz
       {
@@ -503,105 +689,40 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
       for (int i = 0; i < kWarps; ++i) cnnz += S.red_nnz[i];
       cnt = incl[crows - 1];
       if (tid == 0) atomicAdd(&p.ctl->nnz, cnnz);
-      staged = stage != nullptr && cnt <= p.stage_cap;
-      if (staged) {
-        // the chunk's image: every row walked again, runs at its chunk-local offset
-        uint32_t* img = stage + size_t(b) * (p.stage_cap + p.chunk_rows);
-        if (tid == 0) publish_aggregate(p, t, cnt);
-        for (uint32_t r = tid; r < crows; r += kThreads) img[p.stage_cap + r] = incl[r];
-#pragma unroll 1
-        for (int u = 0; u < kWRpt; ++u) {
-          if (uint32_t(u) >= rpt) break;
-          const uint32_t r = (warp * rpt + u) * 32 + lane;
-          if (r >= crows || !((fast_mask >> u) & 1u)) continue;
-          const uint32_t o = r ? incl[r - 1] : 0u;
-          const uint32_t n = incl[r] - o;
-          uint32_t c = 0;
-          unsigned long long z = 0;
-          if (!win_row<A_ID, true>(S, p, uint64_t(c0row) + r, r, c, z, img + o, n))
-            raise_flag(p, &p.ctl->status, 8ull);
-        }
-        if (warp < kWDirectWarps) {
-          for (uint32_t i = warp; i < nslow; i += kWDirectWarps) {
-            const uint32_t r = S.slow[i];
-            const uint32_t o = r ? incl[r - 1] : 0u;
-            const uint32_t n = incl[r] - o;
-            if (n == 0) continue;
-            bool bad = false;
-            const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
-                                          [&](uint64_t k, uint32_t v) {
-                                            if (k < n) img[o + k] = v;
-                                            else bad = true;
-                                          },
-                                          kWDirectWW);
-            if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
-          }
-        }
-        if (nslow_all > uint32_t(kSlowMax)) {
-#pragma unroll 1
-          for (int u = 0; u < kWRpt; ++u) {
-            if (uint32_t(u) >= rpt) break;
-            const uint32_t r = (warp * rpt + u) * 32 + lane;
-            if (r >= crows || ((fast_mask >> u) & 1u)) continue;
-            bool listed = false;
-            for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
-            if (listed) continue;
-            const uint32_t o = r ? incl[r - 1] : 0u;
-            const uint32_t n = incl[r] - o;
-            if (n == 0) continue;
-            const uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
-                                               [&](uint64_t k, uint32_t v) {
-                                                 if (k < n) img[o + k] = v;
-                                               });
-            if (c != n) raise_flag(p, &p.ctl->status, 8ull);
-          }
-        }
-      }
-    }
-    if (tid == 0) S.next = next;
-    // every thread is done with the stages, the run lists, the slow list and
-    // the counted chunk's image
-    cta_sync();
-    const uint32_t tn = S.next;
-    // after a staged chunk the stages are free: the next chunk's operands
-    // are requested phase by phase between the steps of the pending
-    // chunk's write-out, so both latencies overlap
-    const bool pre = have && staged && tn < p.nchunks;
-    const uint32_t n0row = pre ? tn * p.chunk_rows : 0u;
-    const uint32_t ncrows = pre ? min(p.chunk_rows, p.nrows - n0row) : 0u;
-    if (pre) stage_req_rows<A_ID>(S, p, n0row, ncrows);
-    unsigned long long prefix = 0;
-    uint32_t pend_t = 0, pend_crows = 0;
-    unsigned long long pend_cnt = 0;
-    const uint32_t* img = nullptr;
-    if (pend) {
-      pend_t = S.pend_t;
-      pend_crows = S.pend_crows;
-      pend_cnt = S.pend_cnt;
-      prefix = lookback_block(S, p, pend_t, pend_cnt, par);
-      img = stage + size_t(b ^ 1u) * (p.stage_cap + p.chunk_rows);
+      staged = cnt <= p.stage_cap;
     }
     if (pre) stage_rows_req_ranges<A_ID>(S, p, ncrows);
+    if (staged) {
+      // the chunk's image: every row's runs at its chunk-local offset
+      uint32_t* img = stage + size_t(b) * (p.stage_cap + p.chunk_rows);
+      if (tid == 0) publish_aggregate(p, t, cnt);
+      for (uint32_t r = tid; r < crows; r += kThreads) img[p.stage_cap + r] = incl[r];
+      write_rows(c0row, crows, nslow, img, p.stage_cap);
+    }
+    if (pre) stage_window_req_brows<A_ID>(S, p, n0row, ncrows);
     if (pend) {
+      const uint32_t pend_t = S.pend_t[b ^ 1u], pend_crows = S.pend_crows[b ^ 1u];
+      const unsigned long long pend_cnt = S.pend_cnt[b ^ 1u];
+      const unsigned long long prefix = lookback_block(S, p, pend_t, pend_cnt, par);
+      const uint32_t* img = stage + size_t(b ^ 1u) * (p.stage_cap + p.chunk_rows);
       // the pending chunk's row map: loads first, then stores (the staging
       // and the output may alias as far as the compiler knows)
       const uint32_t* pincl = img + p.stage_cap;
       const uint32_t p0row = pend_t * p.chunk_rows;
-      uint32_t v[kWRpt];
+      {
+        uint32_t v[kWRpt];
 #pragma unroll
-      for (int u = 0; u < kWRpt; ++u) {
-        const uint32_t r = tid + u * kThreads;
-        v[u] = r < pend_crows ? __ldcg(pincl + r) : 0u;
-      }
+        for (int u = 0; u < kWRpt; ++u) {
+          const uint32_t r = tid + u * kThreads;
+          v[u] = r < pend_crows ? __ldcg(pincl + r) : 0u;
+        }
 #pragma unroll
-      for (int u = 0; u < kWRpt; ++u) {
-        const uint32_t r = tid + u * kThreads;
-        if (r < pend_crows) p.c_rowmap[uint64_t(p0row) + r + 1] = prefix + v[u];
+        for (int u = 0; u < kWRpt; ++u) {
+          const uint32_t r = tid + u * kThreads;
+          if (r < pend_crows) p.c_rowmap[uint64_t(p0row) + r + 1] = prefix + v[u];
+        }
       }
       if (pend_t == 0 && tid == 0) p.c_rowmap[0] = 0;
-    }
-    if (pre) stage_window_req_brows<A_ID>(S, p, n0row, ncrows);
-    if (pend) {
       // the pending chunk's image: one coalesced copy
       if (prefix + pend_cnt <= p.cap) {
         uint32_t* dst = p.c_entries + prefix;
@@ -625,70 +746,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
       pend = false;
     }
     if (pre) stage_brows_req_branges(S, p);
-    // a counted chunk that was not staged is resolved now, in place, from its
-    // stages (nothing was requested over them)
+    // a counted chunk whose image does not fit the staging: written in place
     if (have && !staged) {
       if (tid == 0) publish_aggregate(p, t, cnt);
       const unsigned long long pfx = lookback_block(S, p, t, cnt, par);
       for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = pfx + incl[r];
       if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
-#pragma unroll 1
-      for (int u = 0; u < kWRpt; ++u) {
-        if (uint32_t(u) >= rpt) break;
-        const uint32_t r = (warp * rpt + u) * 32 + lane;
-        if (r >= crows || !((fast_mask >> u) & 1u)) continue;
-        const unsigned long long dst = pfx + (r ? incl[r - 1] : 0u);
-        const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
-        if (n && dst + n > p.cap) {
-          raise_flag(p, &p.ctl->overflow, 1ull);
-          continue;
-        }
-        uint32_t c = 0;
-        unsigned long long z = 0;
-        if (!win_row<A_ID, true>(S, p, uint64_t(c0row) + r, r, c, z, p.c_entries + dst, n))
-          raise_flag(p, &p.ctl->status, 8ull);
-      }
-      if (warp < kWDirectWarps) {
-        for (uint32_t i = warp; i < nslow; i += kWDirectWarps) {
-          const uint32_t r = S.slow[i];
-          const unsigned long long dst = pfx + (r ? incl[r - 1] : 0u);
-          const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
-          if (n == 0 || dst + n > p.cap) continue;
-          uint32_t* out = p.c_entries + dst;
-          bool bad = false;
-          const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
-                                        [&](uint64_t k, uint32_t v) {
-                                          if (k < n) out[k] = v;
-                                          else bad = true;
-                                        },
-                                        kWDirectWW);
-          if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
-        }
-      }
-      if (nslow_all > uint32_t(kSlowMax)) {
-#pragma unroll 1
-        for (int u = 0; u < kWRpt; ++u) {
-          if (uint32_t(u) >= rpt) break;
-          const uint32_t r = (warp * rpt + u) * 32 + lane;
-          if (r >= crows || ((fast_mask >> u) & 1u)) continue;
-          bool listed = false;
-          for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
-          if (listed) continue;
-          const unsigned long long dst = pfx + (r ? incl[r - 1] : 0u);
-          const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
-          if (n == 0 || dst + n > p.cap) continue;
-          uint32_t* out = p.c_entries + dst;
-          const uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
-                                             [&](uint64_t k, uint32_t v) {
-                                               if (k < n) out[k] = v;
-                                             });
-          if (c != n) raise_flag(p, &p.ctl->status, 8ull);
-        }
-      }
-      cta_sync();  // the stages are read until here
+      write_rows(c0row, crows, nslow, p.c_entries + pfx, p.cap > pfx ? p.cap - pfx : 0ull);
     }
-    // the next chunk was not requested above: stage it now, whole
-    if (!pre && tn < p.nchunks) stage_chunk<A_ID>(S, p, tn);
+    if (tid == 0 && staged) {  // the image just written, in buffer b
+      S.pend_t[b] = t;
+      S.pend_crows[b] = crows;
+      S.pend_cnt[b] = cnt;
+    }
     if (staged) {
       pend = true;
       b ^= 1u;
@@ -697,19 +767,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
     ++iter;
     if (lane == 0) S.phase[warp] = iter;
     if (tid == 0) {
-      if (staged) {
-        S.pend_t = t;
-        S.pend_crows = crows;
-        S.pend_cnt = cnt;
-      }
       S.nslow = 0;
+      S.ngen = 0;
     }
     cta_sync();
     if (warp == 0) {  // one read per lane, one vote
       const bool off = lane < kWarps && S.phase[lane] != iter;
       if (__any_sync(kFullMask, off) && lane == 0) raise_flag(p, &p.ctl->status, 64ull);
     }
-    t = tn;
+    t = have ? tn : 0xffffffffu;
   }
   cp_async_wait();  // nothing may land after the CTA has exited
 }
