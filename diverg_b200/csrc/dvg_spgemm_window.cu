@@ -68,9 +68,10 @@ struct WinSmem {
   uint2 bent[kWBEnt];     // the B window's ranges (from bbase on)
   uint2 frun[kWRows];     // the counted chunk's rows: the run of a one-run row, or a kFrun* marker
   uint32_t list[kWList * kWGenThreads];  // closed runs of the row in hand: entry k of thread t at [k * kWGenThreads + t]
-  // low 16 bits of range offsets (rowmap / 2): A and addend rows c0 .. c0 + crows,
-  // B rows wlo .. wlo + wn; row r spans [rel(x, r), rel(x, r + 1)) of its stage
-  // (16-bit differences: a chunk's rows are used only while it holds < 2^16 ranges)
+  // range offsets (rowmap / 2) relative to the stage's first range, in 16 bits:
+  // A and addend rows c0 .. c0 + crows, B rows wlo .. wlo + wn; row r spans
+  // [x[r], x[r + 1]) of its stage (a chunk's rows are used only while it holds
+  // < 2^16 ranges)
   uint16_t arow[kWRows + 1];
   uint16_t drow[kWRows + 1];
   uint16_t brow[kWBRows + 1];
@@ -108,8 +109,8 @@ static_assert(sizeof(uint2) * kWBEnt >= 8 * (kWBRows + 1), "the B window's row p
 // or are recomputed by the warp path, or by the per-thread bit-window walk.
 constexpr uint32_t kFrunScratch = 0xffffffffu, kFrunWarp = 0xfffffffeu, kFrunLight = 0xfffffffdu;
 
-// Offset of row k's first range from row 0's in a stage of 16-bit words.
-__device__ __forceinline__ uint32_t rel(const uint16_t* x, uint32_t k) { return uint16_t(x[k] - x[0]); }
+// Offset of row k's first range in its stage.
+__device__ __forceinline__ uint32_t rel(const uint16_t* x, uint32_t k) { return x[k]; }
 
 // ---- staging ------------------------------------------------------------------
 // Four phases, each ended by the next one's wait: (1) request the chunk's A
@@ -135,10 +136,6 @@ __device__ void stage_rows_req_ranges(WinSmem& S, const FusedArgs& p, uint32_t c
   const uint64_t* rawD = reinterpret_cast<const uint64_t*>(S.dent);
   cp_async_wait();
   cta_sync();
-  for (uint32_t k = threadIdx.x; k <= crows; k += kThreads) {
-    if (!A_ID) S.arow[k] = uint16_t(rawA[k] >> 1);
-    if (p.d_rowmap) S.drow[k] = uint16_t(rawD[k] >> 1);
-  }
   // every thread reads the same words: the stage sizes are uniform
   uint64_t abase = 0, na64 = 0, dbase = 0, nd64 = 0;
   if (!A_ID) {
@@ -148,6 +145,10 @@ __device__ void stage_rows_req_ranges(WinSmem& S, const FusedArgs& p, uint32_t c
   if (p.d_rowmap) {
     dbase = rawD[0] >> 1;
     nd64 = (rawD[crows] >> 1) - dbase;
+  }
+  for (uint32_t k = threadIdx.x; k <= crows; k += kThreads) {
+    if (!A_ID) S.arow[k] = uint16_t((rawA[k] >> 1) - abase);
+    if (p.d_rowmap) S.drow[k] = uint16_t((rawD[k] >> 1) - dbase);
   }
   const uint32_t na = uint32_t(min(na64, uint64_t(kWAEnt)));
   const uint32_t nd = uint32_t(min(nd64, uint64_t(kWDEnt)));
@@ -238,7 +239,7 @@ __device__ void stage_brows_req_branges(WinSmem& S, const FusedArgs& p) {
     }
     nb64 = (raw[wn] >> 1) - bbase;
   }
-  for (uint32_t k = tid; k <= wn && wn; k += kThreads) S.brow[k] = uint16_t(raw[k] >> 1);
+  for (uint32_t k = tid; k <= wn && wn; k += kThreads) S.brow[k] = uint16_t((raw[k] >> 1) - bbase);
   if (tid == 0) {
     S.wn = wn;
     S.bbase = bbase;
@@ -272,85 +273,81 @@ __device__ void stage_chunk(WinSmem& S, const FusedArgs& p, uint32_t t) {
 // runs kept (a run in frun[r]; two runs in the row's scratch slot `scr`);
 // any other row (more ranges, unstaged data, union levels) returns false and
 // is listed for the general walk, which the CTA spreads over kWGenThreads
-// threads -- a handful of general rows per chunk, so no warp waits on a warp
-// that met one.
+// threads of all warps -- a handful of general rows per chunk, so no warp
+// waits on a warp that met one.
 template <bool A_ID>
 __device__ __forceinline__ bool fast_row(WinSmem& S, const FusedArgs& p, uint32_t row, uint32_t r, uint32_t& count,
                                          unsigned long long& nnz, uint32_t* scr) {
-  const uint32_t rows_ok = S.rows_ok;
-  bool fast = p.nlevels == 0;
+  // the caller checked that the chunk's stages have usable row offsets and
+  // that no union levels are in play
   uint2 u = make_uint2(1u, 0u), v = make_uint2(1u, 0u);  // the row's (at most) two input ranges
+  bool ok = true;
   if (p.d_identity) {
-    u = make_uint2(uint32_t(row), uint32_t(row));
+    u = make_uint2(row, row);
   } else if (p.d_rowmap) {
-    const uint32_t d0 = rel(S.drow, r), d1 = rel(S.drow, r + 1);
-    if (!(rows_ok & 2u) || d1 - d0 > 1u || (d1 > d0 && d0 >= S.nd)) fast = false;
-    else if (d1 > d0) u = S.dent[d0];
+    const uint32_t d0 = S.drow[r], d1 = S.drow[r + 1];
+    ok = d1 - d0 <= 1u && d1 <= S.nd;
+    if (ok && d1 > d0) u = S.dent[d0];
   }
-  uint2 ar;
+  uint2 ar = make_uint2(1u, 0u);
   if (A_ID) {
     ar = id_range(p, row);
   } else {
-    const uint32_t a0 = rel(S.arow, r), a1 = rel(S.arow, r + 1);
-    if (!(rows_ok & 1u) || a1 - a0 != 1u || a0 >= S.na) {
-      fast = false;
-      ar = make_uint2(1u, 0u);
-    } else {
-      ar = S.aent[a0];
+    const uint32_t a0 = S.arow[r], a1 = S.arow[r + 1];
+    ok = ok && a1 - a0 == 1u && a1 <= S.na;
+    if (ok) ar = S.aent[a0];
+  }
+  if (ok && ar.x <= ar.y) {
+    // B rows s..f in the window: f - wlo < wn and s >= wlo (s - wlo <= f - wlo)
+    const uint32_t x = ar.x - S.wlo, y = ar.y - S.wlo;
+    ok = y < S.wn && x <= y;
+    if (ok) {
+      const uint32_t t0 = S.brow[x], t1 = S.brow[y + 1];
+      ok = t1 - t0 <= 1u;
+      if (ok && t1 > t0) v = S.bent[t0];
     }
   }
-  if (fast && ar.x <= ar.y) {
-    const uint32_t wlo = S.wlo;
-    if (ar.x >= wlo && ar.y - wlo < S.wn) {
-      const uint32_t t0 = rel(S.brow, ar.x - wlo), t1 = rel(S.brow, ar.y + 1 - wlo);
-      if (t1 - t0 > 1u) fast = false;
-      else if (t1 > t0) v = S.bent[t0];
-    } else {
-      fast = false;
-    }
+  if (!ok) return false;
+  const bool hu = u.x <= u.y, hv = v.x <= v.y;
+  if (hu && hv && v.x < u.x) {
+    const uint2 w = u;
+    u = v;
+    v = w;
   }
-  if (!fast) return false;
-  {
-    const bool hu = u.x <= u.y, hv = v.x <= v.y;
-    if (hu && hv && v.x < u.x) {
-      const uint2 w = u;
-      u = v;
-      v = w;
-    }
-    uint32_t nr;
-    uint2 r0 = hu ? u : v, r1 = v;
-    if (hu && hv) {
-      if (v.x <= u.y || v.x - u.y == 1u) {  // overlapping or adjacent: one run
-        r0 = make_uint2(u.x, max(u.y, v.y));
-        nr = 1;
-      } else {
-        nr = 2;
-      }
+  uint32_t nr;
+  uint2 r0 = hu ? u : v, r1 = v;
+  if (hu && hv) {
+    if (v.x <= u.y || v.x - u.y == 1u) {  // overlapping or adjacent: one run
+      r0 = make_uint2(u.x, max(u.y, v.y));
+      nr = 1;
     } else {
-      nr = (hu || hv) ? 1u : 0u;
+      nr = 2;
     }
-    if (nr == 2) {
-      *reinterpret_cast<uint4*>(scr) = make_uint4(r0.x, r0.y, r1.x, r1.y);
-      S.frun[r] = make_uint2(kFrunScratch, 0u);
-    } else {
-      S.frun[r] = r0;
-    }
-    count = 2 * nr;
-    nnz += (nr ? uint64_t(r0.y - r0.x) + 1 : 0) + (nr == 2 ? uint64_t(r1.y - r1.x) + 1 : 0);
-    return true;
+  } else {
+    nr = (hu || hv) ? 1u : 0u;
   }
+  if (nr == 2) {
+    *reinterpret_cast<uint4*>(scr) = make_uint4(r0.x, r0.y, r1.x, r1.y);
+    S.frun[r] = make_uint2(kFrunScratch, 0u);
+    nnz += uint64_t(r0.y - r0.x) + uint64_t(r1.y - r1.x) + 2;
+  } else {
+    S.frun[r] = r0;
+    if (nr) nnz += uint64_t(r0.y - r0.x) + 1;
+  }
+  count = 2 * nr;
+  return true;
 }
 
 // The general walk of C row `row` (chunk row r) from the stages (HBM for what
-// is not staged) into the thread's run list (threads < kWGenThreads).
+// is not staged) into run list `slot` (< kWGenThreads) of the walking thread.
 // Returns true with count = the row's entries, its nnz accumulated and its
 // runs kept as fast_row keeps them (more than one run: in its scratch slot
 // `scr`); false, leaving no trace, when the runs overflow the list.
 template <bool A_ID>
 __device__ bool general_row(WinSmem& S, const FusedArgs& p, uint64_t row, uint32_t r, uint32_t& count,
-                            unsigned long long& nnz, uint32_t* scr) {
+                            unsigned long long& nnz, uint32_t* scr, uint32_t slot) {
   constexpr uint32_t kT = kWGenThreads;
-  uint32_t* L = S.list + threadIdx.x;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
+  uint32_t* L = S.list + slot;  // run k: lo at L[2k*kT], hi at L[(2k+1)*kT]
   constexpr uint32_t max_runs = kWList / 2;
   uint32_t nr = 0;
   // merges [x, y] into the list; false when it needs more runs than fit
@@ -596,28 +593,38 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
     unsigned long long nnz_acc = 0, cnt = 0, cnnz = 0;
     uint32_t nslow = 0;
     bool staged = false;
+    uint32_t next = 0xffffffffu;
     if (have) {
-      // the next chunk, taken while this one is counted
-      if (tid == 0) S.next = stopped() ? 0xffffffffu : atomicAdd(p.ticket, 1u);
+      // the next chunk, taken while this one is counted (the ticket's
+      // latency hides behind the rows; it is stored after them)
+      if (tid == 0 && !stopped()) next = atomicAdd(p.ticket, 1u);
       // count: fast rows by their threads, the rest listed
+      const bool try_fast = S.rows_ok == 3u && p.nlevels == 0;
 #pragma unroll 1
       for (int u = 0; u < kWRpt; ++u) {
         if (uint32_t(u) >= rpt) break;
         const uint32_t r = (warp * rpt + u) * 32 + lane;
         if (r < crows) {
           uint32_t c = 0;
-          if (fast_row<A_ID>(S, p, c0row + r, r, c, nnz_acc, scratch + size_t(r) * kWRowScratch)) incl[r] = c;
-          else S.gen[atomicAdd(&S.ngen, 1u)] = uint16_t(r);
+          if (try_fast && fast_row<A_ID>(S, p, c0row + r, r, c, nnz_acc, scratch + size_t(r) * kWRowScratch))
+            incl[r] = c;
+          else
+            S.gen[atomicAdd(&S.ngen, 1u)] = uint16_t(r);
         }
       }
       cta_sync();
-      // the general walk, spread over kWGenThreads threads
+      // the general walk, spread over the warps (lanes < kGenLanes of each):
+      // entry i to warp i % kWarps, so the warps share the few general rows
+      // of a chunk instead of one warp serialising them
       const uint32_t ngen = S.ngen;
-      if (tid < kWGenThreads) {
-        for (uint32_t i = tid; i < ngen; i += kWGenThreads) {
+      constexpr uint32_t kGenLanes = kWGenThreads / kWarps;
+      if (uint32_t(lane) < kGenLanes) {
+        const uint32_t slot = warp * kGenLanes + lane;  // the walker's run list
+        for (uint32_t i = uint32_t(lane) * kWarps + warp; i < ngen; i += kWGenThreads) {
           const uint32_t r = S.gen[i];
           uint32_t c = 0;
-          if (!general_row<A_ID>(S, p, uint64_t(c0row) + r, r, c, nnz_acc, scratch + size_t(r) * kWRowScratch)) {
+          if (!general_row<A_ID>(S, p, uint64_t(c0row) + r, r, c, nnz_acc, scratch + size_t(r) * kWRowScratch,
+                                 slot)) {
             const uint32_t j = atomicAdd(&S.nslow, 1u);
             if (j < uint32_t(kSlowMax)) {
               S.slow[j] = r;
@@ -631,6 +638,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
           incl[r] = c;
         }
       }
+      if (tid == 0) S.next = next;
       cta_sync();
     }
     // the counted chunk's stages are dead: request the next chunk's operands
@@ -690,12 +698,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_window(FusedArgs p) {
       cnt = incl[crows - 1];
       if (tid == 0) atomicAdd(&p.ctl->nnz, cnnz);
       staged = cnt <= p.stage_cap;
+      // later chunks' look-backs wait on this word: published as soon as known
+      if (staged && tid == 0) publish_aggregate(p, t, cnt);
     }
     if (pre) stage_rows_req_ranges<A_ID>(S, p, ncrows);
     if (staged) {
       // the chunk's image: every row's runs at its chunk-local offset
       uint32_t* img = stage + size_t(b) * (p.stage_cap + p.chunk_rows);
-      if (tid == 0) publish_aggregate(p, t, cnt);
       for (uint32_t r = tid; r < crows; r += kThreads) img[p.stage_cap + r] = incl[r];
       write_rows(c0row, crows, nslow, img, p.stage_cap);
     }
