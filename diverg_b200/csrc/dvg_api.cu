@@ -752,9 +752,6 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "row_stage")) {
       require(value == 0 || value == 1, "row_stage must be 0 or 1");
       ctx->opt_row_stage = value;
-    } else if (!std::strcmp(key, "row_window")) {
-      require(value == 0 || value == 1, "row_window must be 0 or 1");
-      ctx->opt_row_window = value;
     } else if (!std::strcmp(key, "row_slot")) {
       require(value >= 0 && value <= 2, "row_slot must be 0 (16 entries), 1 (24) or 2 (32)");
       ctx->opt_row_slot = value;

@@ -190,10 +190,9 @@ uint64_t predict_build_bytes(double growth, uint32_t n, uint64_t nentries, unsig
   const uint64_t est = std::max<uint64_t>(uint64_t(growth * double(nentries)), 4ull * n) + 64;
   const uint64_t slot = 8ull * (uint64_t(n) + 1) + entries_alloc_bytes(est);
   // chunk descriptors, and the row kernel's staging: two buffers of 17 words
-  // a chunk row per resident CTA plus a scratch of 8 words a chunk row -- at
-  // most 168 bytes a row, and at most 42 x 4 bytes x 2048 rows for each of
-  // the 2 CTAs of an SM's 148
-  const uint64_t stage = std::min<uint64_t>(168ull * n, 2ull * 148 * 42 * 4 * 2048);
+  // a chunk row per resident CTA -- at most 136 bytes a row, and at most
+  // 2 x 17 x 4 bytes x 2048 rows for each of the 2 CTAs of an SM's 148
+  const uint64_t stage = std::min<uint64_t>(136ull * n, 2ull * 148 * 2 * 17 * 4 * 2048);
   const uint64_t scratch = plan.steps.size() * ((uint64_t(n) / 64 + 1) * 32 + 512) + stage;
   // the input is held twice while a batch lays it out block-diagonally
   return 2 * input + uint64_t(max_live) * slot + scratch;

@@ -72,8 +72,6 @@ struct dvg_context {
   int64_t opt_row_slot = 1;           // row kernel run-list width variant (0: 16, 1: 24, 2: 32 entries)
   int64_t opt_levels = 1;             // products with long A ranges read union levels of B (row kernel)
   uint32_t row_resident[3] = {0, 0, 0};  // resident CTAs of the row kernel per variant
-  uint32_t win_resident = 0;          // resident CTAs of the window kernel
-  int64_t opt_row_window = 1;         // row products: 1 = the window kernel (operands staged in shared memory)
   int64_t opt_planned = 1;            // 1: index builds run planned (no host round trips)
   double plan_growth = 3.0;           // planned builds: entry capacity per step / input entries
   uint64_t max_product_entries = 0;   // largest product output since the last reset (read-back path)
@@ -209,10 +207,7 @@ struct RowLaunchShape {
 };
 RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_rows_opt, int slot_variant);
 void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& shape);
-// The same product by the window kernel (dvg_spgemm_window.cu): the chunk's A
-// and addend rows and the window of B rows they name staged in shared memory.
-void launch_rowmode_window(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& shape);
-uint32_t window_resident(dvg_context* ctx);
+
 int row_slot_entries(int variant);
 // Runs the row kernel's look-back on descriptors nothing publishes, its wait
 // bounded by spin_limit polls (the kernel records a timeout in the control

@@ -24,7 +24,6 @@ constexpr int kBitWords = 6144;   // union bitmaps (PRE, SUF, BU) or direct wind
 constexpr int kStageMax = 6144;   // output entries staged per chunk
 constexpr int kMaxBlock = 32;     // union block rows (at most a warp)
 constexpr int kSlowMax = 512;     // row mode: rows per chunk deferred to the warp path
-constexpr int kRowScratchPerRow = 8;  // window kernel: scratch entries a chunk row (rows of several runs)
 constexpr int kDirectWW = kBitWords / (2 * kWarps);  // direct path window words per warp
 constexpr int kMaxLevels = 12;    // union levels of B (blocks of up to 4096 rows)
 constexpr unsigned long long kFlag = 1ull << 63;
@@ -318,8 +317,7 @@ __device__ void lookback_warp(const FusedArgs& p, uint32_t t, unsigned long long
   prefix_nnz = pre_nnz;
 }
 
-// ---- pieces of the thread-per-row kernels (dvg_spgemm_rows.cu,
-// dvg_spgemm_window.cu) -------------------------------------------------------------
+// ---- pieces of the thread-per-row kernel (dvg_spgemm_rows.cu) ---------------------
 
 // CTA barrier that counts threads, not warps: the non-aligned form of
 // barrier.sync, which the lanes of a warp may reach at different times.  The

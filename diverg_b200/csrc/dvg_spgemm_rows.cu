@@ -595,7 +595,6 @@ RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_
   }
   RowLaunchShape s{};
   s.resident = ctx->row_resident[v];
-  if (ctx->opt_row_window) s.resident = std::min(s.resident, window_resident(ctx));
   // chunk rows: as large as possible (fewer look-back steps) while keeping
   // about four chunks per resident CTA
   uint32_t chunk_rows = kChunkMax;
@@ -605,8 +604,7 @@ RowLaunchShape row_launch_shape(dvg_context* ctx, uint32_t nrows, int64_t chunk_
   s.nchunks = uint32_t((uint64_t(nrows) + chunk_rows - 1) / chunk_rows);
   s.grid = uint32_t(std::min<uint64_t>(s.nchunks, s.resident));
   s.desc_bytes = size_t(s.nchunks) * sizeof(ChunkDesc);
-  // per CTA two image buffers, then (the window kernel) a scratch for rows of several runs
-  s.stage_bytes = size_t(s.grid) * (2 * (kRowStagePerRow + 1) + kRowScratchPerRow) * s.chunk_rows * sizeof(uint32_t);
+  s.stage_bytes = size_t(s.grid) * 2 * (kRowStagePerRow + 1) * s.chunk_rows * sizeof(uint32_t);
   return s;
 }
 
@@ -635,14 +633,6 @@ void selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit) {
 
 void launch_rowmode(dvg_context* ctx, const RowLaunch& L, const RowLaunchShape& s) {
   if (L.nrows == 0) return;
-  // the window kernel stages with 8-byte asynchronous copies
-  const uintptr_t mis = reinterpret_cast<uintptr_t>(L.a_rowmap) | reinterpret_cast<uintptr_t>(L.a_entries) |
-                        reinterpret_cast<uintptr_t>(L.b_rowmap) | reinterpret_cast<uintptr_t>(L.b_entries) |
-                        reinterpret_cast<uintptr_t>(L.d_rowmap) | reinterpret_cast<uintptr_t>(L.d_entries);
-  if (ctx->opt_row_window && L.nlevels == 0 && L.stage_buf && (mis & 7u) == 0) {
-    launch_rowmode_window(ctx, L, s);
-    return;
-  }
   const int v = std::min(std::max(L.slot_variant, 0), 2);
   FusedArgs p{};
   p.a_rowmap = L.a_identity ? nullptr : L.a_rowmap;
