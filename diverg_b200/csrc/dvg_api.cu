@@ -378,6 +378,37 @@ dvg_matrix* range_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix*
     require(a->nrows <= a->ncols, "range_spadd: identity does not fit the matrix");
   }
   const uint32_t n = a->nrows;
+  // the one-pass kernel stages ranges with 8-byte asynchronous copies
+  const bool aligned = ((reinterpret_cast<uintptr_t>(a->entries) |
+                         reinterpret_cast<uintptr_t>(b_identity ? nullptr : b->entries)) & 7u) == 0;
+  if (ctx->opt_spadd_single && n > 0 && aligned) {
+    // one pass: the output never holds more entries than both inputs
+    const uint64_t cap = a->nentries + (b_identity ? 2ull * n : b->nentries);
+    dvg_matrix* c = new_matrix(ctx, n, a->ncols, cap);
+    void* scratch = nullptr;
+    try {
+      scratch = dalloc(ctx, spadd_single_pass_scratch(n));
+      reset_control(ctx);
+      cudaEvent_t t0 = span_begin(ctx);
+      launch_spadd_single_pass(ctx, a, b, b_identity, c->rowmap, c->entries, cap, scratch);
+      span_end(ctx, t0, kSpadd);
+      const DeviceControl ctl = read_control(ctx);
+      dfree(ctx, scratch);
+      scratch = nullptr;
+      if (ctl.timeout) throw Error(DVG_ERR_TIMEOUT, "range_spadd: chunk look-back wait expired");
+      if (ctl.overflow) throw Error(DVG_ERR_DEVICE, "range_spadd: output capacity overflow");
+      c->nentries = ctl.total;
+      c->nnz = ctl.nnz;
+      c->canonical = a->canonical && (b_identity || b->canonical);
+      ctx->stats.spadd_calls++;
+      ctx->stats.alg_bytes += matrix_bytes(a) + (b_identity ? 0 : matrix_bytes(b)) + matrix_bytes(c);
+    } catch (...) {
+      if (scratch) dfree(ctx, scratch);
+      free_matrix(ctx, c);
+      throw;
+    }
+    return c;
+  }
   dvg_matrix* c = new_matrix(ctx, n, a->ncols, 0);
   try {
     DVG_CUDA(cudaMemsetAsync(c->rowmap, 0, sizeof(uint64_t), ctx->stream));
@@ -752,6 +783,9 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
     } else if (!std::strcmp(key, "row_stage")) {
       require(value == 0 || value == 1, "row_stage must be 0 or 1");
       ctx->opt_row_stage = value;
+    } else if (!std::strcmp(key, "spadd_single")) {
+      require(value == 0 || value == 1, "spadd_single must be 0 or 1");
+      ctx->opt_spadd_single = value;
     } else if (!std::strcmp(key, "row_slot")) {
       require(value >= 0 && value <= 2, "row_slot must be 0 (16 entries), 1 (24) or 2 (32)");
       ctx->opt_row_slot = value;

@@ -71,6 +71,7 @@ struct dvg_context {
   size_t row_stage_cap = 0;           // bytes
   int64_t opt_row_slot = 1;           // row kernel run-list width variant (0: 16, 1: 24, 2: 32 entries)
   int64_t opt_levels = 1;             // products with long A ranges read union levels of B (row kernel)
+  int64_t opt_spadd_single = 1;       // SpAdd: 1 = one pass with a chunk look-back, 0 = count, scan, fill
   uint32_t row_resident[3] = {0, 0, 0};  // resident CTAs of the row kernel per variant
   int64_t opt_planned = 1;            // 1: index builds run planned (no host round trips)
   double plan_growth = 3.0;           // planned builds: entry capacity per step / input entries
@@ -151,6 +152,13 @@ void launch_narrow_rowmap(dvg_context* ctx, const uint64_t* src, uint32_t* dst, 
 void launch_rowmap_scan(dvg_context* ctx, uint64_t* rowmap, uint64_t n);
 void launch_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity, uint64_t* c_rowmap,
                   uint32_t* c_entries, bool fill);
+// C = A + B (B the identity when b_identity) in one pass: c_rowmap written
+// fully, c_entries up to `cap` entries (a.nentries + b's entries always
+// suffice); the control block receives the total entries, the nnz and a
+// timeout flag.  `scratch`: spadd_single_pass_scratch(a->nrows) bytes.
+uint64_t spadd_single_pass_scratch(uint32_t nrows);
+void launch_spadd_single_pass(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bool b_identity,
+                              uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap, void* scratch);
 // Out-of-range pairs are counted into ctl->invalid (ctx->d_ctl when null).
 void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out,
                   DeviceControl* ctl = nullptr);

@@ -455,3 +455,55 @@ def test_reference_api_mirror():
         assert_same(p, want.rowmap, want.entries, want.nnz)
         pairs = gen.query_pairs(a, 1000, 0.5, 10, 30)
         assert np.array_equal(dv.query_batch(idx, pairs), orc.query(omat(idx), pairs))
+
+
+def _noncanonical(m, split_every=1):
+    """m with the first multi-column range of every row split into two
+    adjacent ranges, and every third row's first range repeated."""
+    out_e, out_r = [], [0]
+    for i in range(m.numRows()):
+        e = m.entries[int(m.rowmap[i]):int(m.rowmap[i + 1])].tolist()
+        split = False
+        row = []
+        for k in range(0, len(e), 2):
+            if not split and e[k + 1] > e[k] and i % split_every == 0:
+                row += [e[k], e[k], e[k] + 1, e[k + 1]]
+                split = True
+            else:
+                row += [e[k], e[k + 1]]
+        if i % 3 == 0 and row:
+            row = row[:2] + row
+        out_e += row
+        out_r.append(len(out_e))
+    return CRSMatrix(m.numCols(), np.array(out_e, np.uint32), np.array(out_r, np.uint64))
+
+
+@pytest.mark.parametrize("single", [1, 0])
+@pytest.mark.parametrize("shape", ["banded", "wide_rows", "noncanonical", "empty_rows", "one_row"])
+def test_spadd_one_pass_and_three_pass(ctx, single, shape):
+    # range_spadd (range_sparse.hpp:112-477) in one pass with a chunk look-back
+    # and by count, scan and fill: rows past the per-chunk stages (wide rows),
+    # chunks whose output exceeds the shared image, the reference's merge on
+    # non-canonical rows (tails copied verbatim), empty rows
+    if shape == "banded":
+        a = gen.banded(300_000, 512, 4.0, 32.0, seed=301)
+        b = gen.banded(300_000, 512, 4.0, 32.0, seed=302)
+    elif shape == "wide_rows":
+        a = gen.banded(20_000, 4000, 12.0, 2.0, seed=303)
+        b = gen.banded(20_000, 4000, 12.0, 2.0, seed=304)
+    elif shape == "noncanonical":
+        a = _noncanonical(gen.random_matrix(3000, 20_000, seed=305))
+        b = _noncanonical(gen.random_matrix(3000, 20_000, seed=306), split_every=2)
+    elif shape == "empty_rows":
+        a = gen.random_matrix(50_000, 5_000, seed=307)
+        b = gen.random_matrix(50_000, 3_000, seed=308)
+    else:
+        a = CRSMatrix(9, np.array([0, 3, 5, 8], np.uint32), np.array([0, 4], np.uint64))
+        b = CRSMatrix(9, np.array([4, 4], np.uint32), np.array([0, 2], np.uint64))
+    want = orc.spadd(omat(a), omat(b))
+    ctx.set_option("spadd_single", single)
+    try:
+        got = ctx.spadd(ctx.upload(a), ctx.upload(b)).download()
+    finally:
+        ctx.set_option("spadd_single", 1)
+    assert_same(got, want.rowmap, want.entries, want.nnz, shape)
