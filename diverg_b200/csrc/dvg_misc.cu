@@ -253,30 +253,38 @@ __global__ void __launch_bounds__(kThreads) k_spadd(SpaddArgs p) {
 }
 
 // ---- SpAdd in one pass ----------------------------------------------------------
-// The same rows as k_spadd (spadd_row), with no counting pass and no scan: a
-// persistent CTA takes chunks of kThreads rows from a ticket, copies the
-// chunk's row pointers and ranges of A and B -- contiguous in HBM -- into
-// shared memory with asynchronous copies, merges a row per thread (count),
-// takes the chunk-local prefix, publishes the chunk's entry count for later
-// chunks, merges again into a shared image of the chunk's output, finds its
-// offset by a decoupled look-back over earlier chunks' descriptors, and
-// writes the chunk's row map and entries with coalesced stores.  Rows whose
-// ranges lie past the stages read HBM; a chunk whose output exceeds the image
-// is written straight to C.  Reads A and B once, writes C once.
-constexpr int kAddStage = 1536;          // ranges of each operand staged per chunk
-constexpr int kAddImage = 4 * kAddStage;  // output entries a chunk keeps in shared memory
+// The same rows as k_spadd (the merge of spadd_row), with no counting pass and
+// no scan: a persistent CTA takes chunks of kAddThreads rows from a ticket,
+// copies the chunk's row pointers and ranges of A and B -- contiguous in HBM --
+// into shared memory with asynchronous copies, merges a row per thread
+// (count), takes the chunk-local prefix, publishes the chunk's entry count
+// for later chunks' look-backs and merges again into a shared image of the
+// chunk's output.  The image waits in shared memory (two buffers) and is
+// resolved one iteration later: by then the chunks before it have long
+// published their counts, so its decoupled look-back rarely waits, and it is
+// written out with coalesced stores.  Rows whose ranges lie past the stages
+// read HBM; a chunk whose output exceeds its image buffer is resolved and
+// written straight to C in its own iteration.  Reads A and B once, writes C
+// once.
+constexpr int kAddThreads = 128;
+constexpr int kAddStage = 6 * kAddThreads;   // ranges of each operand staged per chunk
+constexpr int kAddImage = 16 * kAddThreads;  // output entries of a chunk held in an image buffer
 constexpr unsigned long long kAddFlag = 1ull << 63;
 constexpr uint32_t kAddSpinLimit = 1u << 22;
 
 struct AddSmem {
   uint2 a[kAddStage];
   uint2 b[kAddStage];
-  uint32_t img[kAddImage];
-  unsigned long long arow[kThreads + 1];  // the chunk's row pointers (entry offsets)
-  unsigned long long brow[kThreads + 1];
-  uint32_t wsum[kThreads / 32];
-  unsigned long long wnnz[kThreads / 32];
-  unsigned long long prefix;
+  uint32_t img[2][kAddImage];             // images of the counted and the pending chunk
+  uint32_t incl[2][kAddThreads];          // their chunk-local inclusive row counts
+  unsigned long long arow[kAddThreads + 1];  // the chunk's row pointers (entry offsets)
+  unsigned long long brow[kAddThreads + 1];
+  uint32_t wsum[kAddThreads / 32];
+  unsigned long long wnnz[kAddThreads / 32];
+  unsigned long long prefix[2];           // exclusive prefixes: the pending chunk's, a chunk written in place
+  // the pending chunk (in buffer k), per buffer: its readers and the writer of
+  // the next one never meet on one slot
+  uint32_t pend_t[2], pend_rows[2], pend_cnt[2];
   uint32_t next;
 };
 
@@ -307,153 +315,198 @@ struct SpaddChunkArgs {
   uint32_t spin_limit;       // polls a look-back waits before it gives up (0: kAddSpinLimit)
 };
 
+// Warp 0 walks back from chunk t (whose aggregate is published) to the
+// nearest inclusive prefix, publishes t's inclusive prefix and leaves t's
+// exclusive prefix in *out (shared); the caller's barrier makes it visible.
+__device__ void add_lookback(unsigned long long* out, const SpaddChunkArgs& p, uint32_t t, uint32_t cnt) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long pre = 0;
+  int64_t j = int64_t(t) - 1;
+  uint32_t spins = 0;
+  const uint32_t limit = p.spin_limit ? p.spin_limit : kAddSpinLimit;
+  while (j >= 0) {
+    const int64_t idx = j - lane;
+    int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: nothing yet
+    unsigned long long v = 0;
+    if (idx >= 0) {
+      unsigned long long va, vi;
+      asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
+                   : "=l"(va), "=l"(vi) : "l"(p.desc + 2 * size_t(idx)) : "memory");
+      if (vi & kAddFlag) {
+        v = vi & ~kAddFlag;
+      } else if (va & kAddFlag) {
+        st = 1;
+        v = va & ~kAddFlag;
+      } else {
+        st = 0;
+      }
+    }
+    const unsigned im = __ballot_sync(kFullMask, st == 2), wm = __ballot_sync(kFullMask, st == 0);
+    const int fi = im ? __ffs(im) - 1 : 32;
+    const unsigned before = fi == 32 ? kFullMask : ((1u << fi) - 1u);
+    if (wm & before) {
+      if (++spins > limit) {
+        if (lane == 0) atomicOr(&p.ctl->timeout, 1ull);  // the wait ran out
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    unsigned long long sv = lane <= fi ? v : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(kFullMask, sv, o);
+    pre += sv;
+    if (fi < 32) break;
+    j -= 32;
+  }
+  if (lane == 0) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p.desc + 2 * size_t(t) + 1), "l"(kAddFlag | (pre + cnt))
+                 : "memory");
+    *out = pre;
+    if (t == p.nchunks - 1) p.ctl->total = pre + cnt;
+  }
+}
+
 template <bool B_ID>
-__global__ void __launch_bounds__(kThreads) k_spadd_chunks(SpaddChunkArgs p) {
+__global__ void __launch_bounds__(kAddThreads) k_spadd_chunks(SpaddChunkArgs p) {
   extern __shared__ __align__(16) unsigned char add_smem_raw[];
   AddSmem& S = *reinterpret_cast<AddSmem*>(add_smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned long long nnz_cta = 0;
   if (tid == 0) S.next = atomicAdd(p.ticket, 1u);
   add_sync();
-  uint32_t t = S.next;
-  while (t < p.nchunks) {
-    const uint32_t c0 = t * uint32_t(kThreads);
-    const uint32_t crows = min(uint32_t(kThreads), p.nrows - c0);
-    // 1. the chunk's row pointers
-    for (uint32_t k = tid; k <= crows; k += kThreads) {
-      add_cp8(&S.arow[k], p.a_rowmap + uint64_t(c0) + k);
-      if (!B_ID) add_cp8(&S.brow[k], p.b_rowmap + uint64_t(c0) + k);
-    }
-    add_cp_wait();
-    add_sync();
-    const uint64_t abase = S.arow[0], bbase = B_ID ? 0 : S.brow[0];
-    const uint64_t ra = (S.arow[crows] - abase) / 2, rb = B_ID ? 0 : (S.brow[crows] - bbase) / 2;
-    const uint32_t nas = ra < uint64_t(kAddStage) ? uint32_t(ra) : uint32_t(kAddStage);
-    const uint32_t nbs = rb < uint64_t(kAddStage) ? uint32_t(rb) : uint32_t(kAddStage);
-    // 2. their ranges (rows start at even entries: a range is one 8-byte copy)
-    for (uint32_t k = tid; k < nas; k += kThreads) add_cp8(&S.a[k], p.a_entries + abase + 2 * uint64_t(k));
-    for (uint32_t k = tid; k < nbs; k += kThreads) add_cp8(&S.b[k], p.b_entries + bbase + 2 * uint64_t(k));
-    if (tid == 0) S.next = atomicAdd(p.ticket, 1u);  // the next chunk, while the ranges land
-    add_cp_wait();
-    add_sync();
-    // 3. count this thread's row
+  uint32_t t = S.next, b = 0;
+  bool pend = false;  // a counted chunk waits in image buffer b ^ 1
+  while (t < p.nchunks || pend) {
+    const bool have = t < p.nchunks;
+    const uint32_t c0 = have ? t * uint32_t(kAddThreads) : 0u;
+    const uint32_t crows = have ? min(uint32_t(kAddThreads), p.nrows - c0) : 0u;
+    uint32_t cnt = 0, excl = 0, cnt_r = 0;
+    bool imaged = false;
+    const uint2* ap = nullptr;
+    const uint2* bp = nullptr;
+    uint32_t na = 0, nb = 0;  // ranges of this thread's row
+    uint2 id;
     const uint32_t r = tid;
     const bool has = r < crows;
-    const uint32_t* ap = nullptr;
-    const uint32_t* bp = nullptr;
-    uint64_t na = 0, nb = 0;
-    uint32_t id[2];
-    if (has) {
-      const uint64_t a0 = S.arow[r] - abase, a1 = S.arow[r + 1] - abase;
-      na = a1 - a0;
-      ap = a1 <= 2ull * nas ? reinterpret_cast<const uint32_t*>(S.a) + a0 : p.a_entries + abase + a0;
-      if (B_ID) {
-        id[0] = id[1] = c0 + r;
-        bp = id;
-        nb = 2;
-      } else {
-        const uint64_t b0 = S.brow[r] - bbase, b1 = S.brow[r + 1] - bbase;
-        nb = b1 - b0;
-        bp = b1 <= 2ull * nbs ? reinterpret_cast<const uint32_t*>(S.b) + b0 : p.b_entries + bbase + b0;
+    if (have) {
+      // 1. the chunk's row pointers
+      for (uint32_t k = tid; k <= crows; k += kAddThreads) {
+        add_cp8(&S.arow[k], p.a_rowmap + uint64_t(c0) + k);
+        if (!B_ID) add_cp8(&S.brow[k], p.b_rowmap + uint64_t(c0) + k);
       }
-    }
-    uint32_t cnt_r = 0;
-    if (has)
-      spadd_row(ap, na, bp, nb, [&](uint32_t lo, uint32_t hi) {
-        cnt_r += 2;
-        nnz_cta += uint64_t(hi) - lo + 1;
-      });
-    // 4. chunk-local prefix
-    uint32_t incl = cnt_r;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t u = __shfl_up_sync(kFullMask, incl, o);
-      if (lane >= o) incl += u;
-    }
-    if (lane == 31) S.wsum[warp] = incl;
-    add_sync();
-    uint32_t wpre = 0, cnt = 0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) {
-      const uint32_t v = S.wsum[w];
-      if (w < warp) wpre += v;
-      cnt += v;
-    }
-    const uint32_t excl = wpre + incl - cnt_r;
-    // 5. the aggregate, as soon as it is known
-    if (tid == 0) {
-      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p.desc + 2 * size_t(t)), "l"(kAddFlag | cnt) : "memory");
-    }
-    const bool imaged = cnt <= uint32_t(kAddImage);
-    if (imaged && has)
-      spadd_row(ap, na, bp, nb, [&, k = excl](uint32_t lo, uint32_t hi) mutable {
-        S.img[k] = lo;
-        S.img[k + 1] = hi;
-        k += 2;
-      });
-    // 6. look-back (warp 0): sum aggregates back to the nearest inclusive prefix
-    if (warp == 0) {
-      unsigned long long pre = 0;
-      int64_t j = int64_t(t) - 1;
-      uint32_t spins = 0;
-      const uint32_t limit = p.spin_limit ? p.spin_limit : kAddSpinLimit;
-      while (j >= 0) {
-        const int64_t idx = j - lane;
-        int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: nothing yet
-        unsigned long long v = 0;
-        if (idx >= 0) {
-          unsigned long long va, vi;
-          asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
-                       : "=l"(va), "=l"(vi) : "l"(p.desc + 2 * size_t(idx)) : "memory");
-          if (vi & kAddFlag) v = vi & ~kAddFlag;
-          else if (va & kAddFlag) { st = 1; v = va & ~kAddFlag; }
-          else st = 0;
+      add_cp_wait();
+      add_sync();
+      const uint64_t abase = S.arow[0], bbase = B_ID ? 0 : S.brow[0];
+      const uint64_t ra = (S.arow[crows] - abase) / 2, rb = B_ID ? 0 : (S.brow[crows] - bbase) / 2;
+      const uint32_t nas = ra < uint64_t(kAddStage) ? uint32_t(ra) : uint32_t(kAddStage);
+      const uint32_t nbs = rb < uint64_t(kAddStage) ? uint32_t(rb) : uint32_t(kAddStage);
+      // 2. their ranges (rows start at even entries: a range is one 8-byte copy)
+      for (uint32_t k = tid; k < nas; k += kAddThreads) add_cp8(&S.a[k], p.a_entries + abase + 2 * uint64_t(k));
+      if (!B_ID)
+        for (uint32_t k = tid; k < nbs; k += kAddThreads) add_cp8(&S.b[k], p.b_entries + bbase + 2 * uint64_t(k));
+      add_cp_wait();
+      add_sync();
+      // 3. count this thread's row
+      if (has) {
+        const uint64_t a0 = (S.arow[r] - abase) / 2, a1 = (S.arow[r + 1] - abase) / 2;
+        na = uint32_t(a1 - a0);
+        ap = a1 <= nas ? S.a + a0 : reinterpret_cast<const uint2*>(p.a_entries + abase) + a0;
+        if (B_ID) {
+          id = make_uint2(c0 + r, c0 + r);
+          bp = &id;
+          nb = 1;
+        } else {
+          const uint64_t b0 = (S.brow[r] - bbase) / 2, b1 = (S.brow[r + 1] - bbase) / 2;
+          nb = uint32_t(b1 - b0);
+          bp = b1 <= nbs ? S.b + b0 : reinterpret_cast<const uint2*>(p.b_entries + bbase) + b0;
         }
-        const unsigned im = __ballot_sync(kFullMask, st == 2), wm = __ballot_sync(kFullMask, st == 0);
-        const int fi = im ? __ffs(im) - 1 : 32;
-        const unsigned before = fi == 32 ? kFullMask : ((1u << fi) - 1u);
-        if (wm & before) {
-          if (++spins > limit) {
-            if (lane == 0) atomicOr(&p.ctl->timeout, 1ull);  // the wait ran out
-            break;
-          }
-          __nanosleep(32);
-          continue;
-        }
-        unsigned long long sv = lane <= fi ? v : 0ull;
+        spadd_row(reinterpret_cast<const uint32_t*>(ap), 2ull * na, reinterpret_cast<const uint32_t*>(bp), 2ull * nb, [&](uint32_t lo, uint32_t hi) {
+          cnt_r += 2;
+          nnz_cta += uint64_t(hi - lo) + 1;
+        });
+      }
+      // 4. chunk-local prefix; the aggregate for later chunks at once
+      uint32_t incl = cnt_r;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(kFullMask, sv, o);
-        pre += sv;
-        if (fi < 32) break;
-        j -= 32;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(kFullMask, incl, o);
+        if (lane >= o) incl += u;
       }
-      if (lane == 0) {
-        asm volatile("st.relaxed.gpu.global.u64 [%0], %1;"
-                     ::"l"(p.desc + 2 * size_t(t) + 1), "l"(kAddFlag | (pre + cnt)) : "memory");
-        S.prefix = pre;
-        if (t == p.nchunks - 1) p.ctl->total = pre + cnt;
+      if (lane == 31) S.wsum[warp] = incl;
+      add_sync();
+      uint32_t wpre = 0;
+#pragma unroll
+      for (int w = 0; w < kAddThreads / 32; ++w) {
+        const uint32_t v = S.wsum[w];
+        if (w < warp) wpre += v;
+        cnt += v;
+      }
+      excl = wpre + incl - cnt_r;
+      if (tid == 0) {
+        asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p.desc + 2 * size_t(t)), "l"(kAddFlag | cnt)
+                     : "memory");
+        S.next = atomicAdd(p.ticket, 1u);  // the next chunk, taken once this one is counted
+      }
+      // 5. the chunk's image in buffer b (its inclusive row counts beside it)
+      imaged = cnt <= uint32_t(kAddImage);
+      if (imaged) {
+        S.incl[b][r] = excl + cnt_r;
+        if (has)
+          spadd_row(reinterpret_cast<const uint32_t*>(ap), 2ull * na, reinterpret_cast<const uint32_t*>(bp), 2ull * nb, [&, k = excl](uint32_t lo, uint32_t hi) mutable {
+            S.img[b][k] = lo;
+            S.img[b][k + 1] = hi;
+            k += 2;
+          });
       }
     }
+    // 6. the pending chunk (counted last iteration): look-back, row map, entries
+    if (pend) {
+      const uint32_t pt = S.pend_t[b ^ 1u], prow = S.pend_rows[b ^ 1u], pcnt = S.pend_cnt[b ^ 1u];
+      if (warp == 0) add_lookback(&S.prefix[0], p, pt, pcnt);
+      add_sync();
+      const unsigned long long prefix = S.prefix[0];
+      if (uint32_t(tid) < prow) p.c_rowmap[uint64_t(pt) * kAddThreads + tid + 1] = prefix + S.incl[b ^ 1u][tid];
+      if (pt == 0 && tid == 0) p.c_rowmap[0] = 0;
+      if (prefix + pcnt <= p.cap) {
+        uint32_t* dst = p.c_entries + prefix;
+        for (uint32_t k = tid; k < pcnt; k += kAddThreads) dst[k] = S.img[b ^ 1u][k];
+      } else if (tid == 0 && pcnt) {
+        atomicOr(&p.ctl->overflow, 1ull);
+      }
+      pend = false;
+    }
+    // 7. a chunk whose output does not fit its image: resolved now, in place
+    if (have && !imaged) {
+      if (warp == 0) add_lookback(&S.prefix[1], p, t, cnt);
+      add_sync();
+      const unsigned long long prefix = S.prefix[1];
+      if (has) p.c_rowmap[uint64_t(c0) + r + 1] = prefix + excl + cnt_r;
+      if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
+      if (prefix + cnt > p.cap) {
+        if (tid == 0 && cnt) atomicOr(&p.ctl->overflow, 1ull);
+      } else if (has) {
+        uint32_t* dst = p.c_entries + prefix + excl;
+        spadd_row(reinterpret_cast<const uint32_t*>(ap), 2ull * na, reinterpret_cast<const uint32_t*>(bp), 2ull * nb, [&, k = 0u](uint32_t lo, uint32_t hi) mutable {
+          dst[k] = lo;
+          dst[k + 1] = hi;
+          k += 2;
+        });
+      }
+    }
+    if (have && imaged) {
+      if (tid == 0) {
+        S.pend_t[b] = t;
+        S.pend_rows[b] = crows;
+        S.pend_cnt[b] = cnt;
+      }
+      pend = true;
+      b ^= 1u;
+    }
+    // every thread is done with the stages and the images it needs; S.next
+    // (written after the prefix) and the pending record are visible
     add_sync();
-    const unsigned long long prefix = S.prefix;
-    // 7. the chunk's row map and entries
-    if (has) p.c_rowmap[uint64_t(c0) + r + 1] = prefix + excl + cnt_r;
-    if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
-    if (prefix + cnt > p.cap) {
-      if (tid == 0 && cnt) atomicOr(&p.ctl->overflow, 1ull);
-    } else if (imaged) {
-      uint32_t* dst = p.c_entries + prefix;
-      for (uint32_t k = tid; k < cnt; k += kThreads) dst[k] = S.img[k];
-    } else if (has) {
-      uint32_t* dst = p.c_entries + prefix + excl;
-      spadd_row(ap, na, bp, nb, [&, k = 0u](uint32_t lo, uint32_t hi) mutable {
-        dst[k] = lo;
-        dst[k + 1] = hi;
-        k += 2;
-      });
-    }
-    t = S.next;
-    add_sync();  // everyone has read S.next and the stages before they are reused
+    t = have ? S.next : 0xffffffffu;
   }
   // the product's nnz: one atomic per CTA
 #pragma unroll
@@ -462,7 +515,7 @@ __global__ void __launch_bounds__(kThreads) k_spadd_chunks(SpaddChunkArgs p) {
   add_sync();
   if (tid == 0) {
     unsigned long long s = 0;
-    for (int w = 0; w < kThreads / 32; ++w) s += S.wnnz[w];
+    for (int w = 0; w < kAddThreads / 32; ++w) s += S.wnnz[w];
     atomicAdd(&p.ctl->nnz, s);
   }
 }
@@ -578,7 +631,7 @@ void launch_spadd(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, bo
 }
 
 uint64_t spadd_single_pass_scratch(uint32_t nrows) {
-  const uint64_t nchunks = (uint64_t(nrows) + kThreads - 1) / kThreads;
+  const uint64_t nchunks = (uint64_t(nrows) + kAddThreads - 1) / kAddThreads;
   return nchunks * 16 + 256;
 }
 
@@ -586,7 +639,7 @@ void launch_spadd_single_pass(dvg_context* ctx, const dvg_matrix* a, const dvg_m
                               uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap, void* scratch) {
   const uint32_t n = a->nrows;
   if (n == 0) return;
-  const uint32_t nchunks = uint32_t((uint64_t(n) + kThreads - 1) / kThreads);
+  const uint32_t nchunks = uint32_t((uint64_t(n) + kAddThreads - 1) / kAddThreads);
   // per chunk 16 bytes of descriptors, then the ticket
   DVG_CUDA(cudaMemsetAsync(scratch, 0, spadd_single_pass_scratch(n), ctx->stream));
   SpaddChunkArgs p{};
@@ -606,10 +659,10 @@ void launch_spadd_single_pass(dvg_context* ctx, const dvg_matrix* a, const dvg_m
   DVG_CUDA(cudaFuncSetAttribute(k_spadd_chunks<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DVG_CUDA(cudaFuncSetAttribute(k_spadd_chunks<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
-  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spadd_chunks<false>, kThreads, smem));
+  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spadd_chunks<false>, kAddThreads, smem));
   const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(std::max(per_sm, 1)) * ctx->num_sms)));
-  if (b_identity) k_spadd_chunks<true><<<grid, kThreads, smem, ctx->stream>>>(p);
-  else k_spadd_chunks<false><<<grid, kThreads, smem, ctx->stream>>>(p);
+  if (b_identity) k_spadd_chunks<true><<<grid, kAddThreads, smem, ctx->stream>>>(p);
+  else k_spadd_chunks<false><<<grid, kAddThreads, smem, ctx->stream>>>(p);
   DVG_CUDA(cudaGetLastError());
   ctx->stats.kernel_launches++;
 }
