@@ -553,6 +553,83 @@ __global__ void __launch_bounds__(kThreads) k_query(const uint64_t* __restrict__
   if (bad) atomicAdd(&ctl->invalid, bad);
 }
 
+// Four consecutive pairs a thread, their loads interleaved: the pairs (two
+// 16-byte loads), the four rows' bounds, then -- for rows of at most two
+// ranges, nearly all rows of an index -- each row's entries in two 8-byte
+// loads, searched in registers by the same binary search as k_query (so the
+// answers are the same on any row, sorted or not); longer rows search HBM.
+// The four answers go out as one 4-byte store.
+__device__ __forceinline__ uint32_t pick4(uint2 e0, uint2 e1, uint64_t k) {
+  return k == 0 ? e0.x : k == 1 ? e0.y : k == 2 ? e1.x : e1.y;
+}
+
+__global__ void __launch_bounds__(kThreads) k_query4(const uint64_t* __restrict__ rowmap,
+                                                     const uint32_t* __restrict__ entries, uint32_t nrows,
+                                                     uint32_t ncols, const uint4* __restrict__ pairs, uint64_t ngroups,
+                                                     uchar4* __restrict__ out, DeviceControl* ctl) {
+  unsigned long long bad = 0;
+  for (uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; g < ngroups;
+       g += uint64_t(gridDim.x) * blockDim.x) {
+    const uint4 p01 = __ldg(pairs + 2 * g), p23 = __ldg(pairs + 2 * g + 1);
+    const uint32_t qi[4] = {p01.x, p01.z, p23.x, p23.z}, qj[4] = {p01.y, p01.w, p23.y, p23.w};
+    bool ok[4];
+    uint64_t lo[4], hi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ok[k] = qi[k] < nrows && qj[k] < ncols;
+      bad += ok[k] ? 0 : 1;
+      lo[k] = ok[k] ? __ldg(rowmap + qi[k]) : 0;
+      hi[k] = ok[k] ? __ldg(rowmap + qi[k] + 1) : 0;
+    }
+    uint2 e0[4], e1[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint64_t len = hi[k] - lo[k];
+      e0[k] = e1[k] = make_uint2(0u, 0u);
+      if (len > 0 && len <= 4) {
+        e0[k] = __ldg(reinterpret_cast<const uint2*>(entries + lo[k]));
+        if (len > 2) e1[k] = __ldg(reinterpret_cast<const uint2*>(entries + lo[k] + 2));
+      }
+    }
+    uint8_t ans[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint64_t n = hi[k] - lo[k];
+      const uint32_t j = qj[k];
+      uint64_t first = 0, len = n;
+      if (n <= 4) {
+        while (len > 0) {
+          const uint64_t half = len >> 1;
+          if (pick4(e0[k], e1[k], first + half) < j) {
+            first += half + 1;
+            len -= half + 1;
+          } else {
+            len = half;
+          }
+        }
+        if (first & 1) --first;
+        ans[k] = (first != n && pick4(e0[k], e1[k], first) <= j) ? 1 : 0;
+      } else {
+        const uint32_t* e = entries + lo[k];
+        while (len > 0) {
+          const uint64_t half = len >> 1;
+          if (__ldg(e + first + half) < j) {
+            first += half + 1;
+            len -= half + 1;
+          } else {
+            len = half;
+          }
+        }
+        if (first & 1) --first;
+        ans[k] = (first != n && __ldg(e + first) <= j) ? 1 : 0;
+      }
+      if (!ok[k]) ans[k] = 0;
+    }
+    out[g] = make_uchar4(ans[0], ans[1], ans[2], ans[3]);
+  }
+  if (bad) atomicAdd(&ctl->invalid, bad);
+}
+
 }  // namespace
 
 void launch_identity(dvg_context* ctx, dvg_matrix* out) {
@@ -670,11 +747,28 @@ void launch_spadd_single_pass(dvg_context* ctx, const dvg_matrix* a, const dvg_m
 void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pairs, uint64_t npairs, uint8_t* d_out,
                   DeviceControl* ctl) {
   if (npairs == 0) return;
-  k_query<<<grid_for(ctx, npairs, kThreads, 16), kThreads, 0, ctx->stream>>>(
-      idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint2*>(d_pairs), npairs, d_out,
-      ctl ? ctl : ctx->d_ctl);
-  DVG_CUDA(cudaGetLastError());
-  ctx->stats.kernel_launches++;
+  DeviceControl* c = ctl ? ctl : ctx->d_ctl;
+  // four pairs a thread when the buffers allow 16-byte pair loads and
+  // 4-byte answer stores; the last npairs % 4 pairs (or all) one a thread
+  uint64_t done = 0;
+  const bool vec = ((reinterpret_cast<uintptr_t>(d_pairs) & 15u) | (reinterpret_cast<uintptr_t>(d_out) & 3u) |
+                    (reinterpret_cast<uintptr_t>(idx->entries) & 7u)) == 0;
+  if (vec && npairs >= 4) {
+    const uint64_t groups = npairs / 4;
+    k_query4<<<grid_for(ctx, groups, kThreads, 8), kThreads, 0, ctx->stream>>>(
+        idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint4*>(d_pairs), groups,
+        reinterpret_cast<uchar4*>(d_out), c);
+    DVG_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
+    done = 4 * groups;
+  }
+  if (done < npairs) {
+    k_query<<<grid_for(ctx, npairs - done, kThreads, 16), kThreads, 0, ctx->stream>>>(
+        idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint2*>(d_pairs) + done,
+        npairs - done, d_out + done, c);
+    DVG_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
+  }
 }
 
 }  // namespace dvg

@@ -507,3 +507,43 @@ def test_spadd_one_pass_and_three_pass(ctx, single, shape):
     finally:
         ctx.set_option("spadd_single", 1)
     assert_same(got, want.rowmap, want.entries, want.nnz, shape)
+
+
+@pytest.mark.parametrize("npairs", [1, 3, 4, 4097, 200_001])
+@pytest.mark.parametrize("offset", [0, 1, 2])
+def test_query_paths_and_tails(ctx, npairs, offset):
+    # membership queries (crs_matrix.hpp:149-169) by the four-pairs-a-thread
+    # kernel and the one-pair kernel: counts that leave a tail, pair and answer
+    # buffers offset so the four-pair path does not apply, rows of one to many
+    # ranges, a non-canonical row set, out-of-range pairs answered 0
+    import torch
+    a = gen.random_matrix(5000, 60_000, seed=331)  # rows of ~12 ranges and rows of few
+    m = _noncanonical(a, split_every=3)
+    d = ctx.upload(m)
+    rng = np.random.default_rng(npairs + offset)
+    pairs = np.stack([rng.integers(0, 5000, npairs + offset), rng.integers(0, 5000, npairs + offset)], 1)
+    pairs = pairs.astype(np.uint32)
+    want = orc.query(omat(m), pairs[offset:])
+    d_pairs = torch.from_numpy(pairs.view(np.int32).reshape(-1)).cuda()
+    d_out = torch.zeros(npairs + offset, dtype=torch.uint8, device="cuda")
+    ctx.query_device(d, d_pairs.data_ptr() + 8 * offset, npairs, d_out.data_ptr() + offset)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_out.cpu().numpy()[offset:], want)
+    # the same through host buffers
+    assert np.array_equal(ctx.query(d, pairs[offset:]), want)
+
+
+def test_query_out_of_range_pairs_answer_zero_in_both_paths(ctx):
+    import torch
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(20_000, seed=332))
+    d = ctx.upload(a)
+    n = a.numRows()
+    pairs = np.array([[0, 1], [n, 0], [1, n + 5], [2, 3], [5, 6], [n + 1, n + 1], [7, 8], [9, 10]], np.uint32)
+    want = orc.query(omat(a), np.where(pairs < n, pairs, 0).astype(np.uint32))
+    want[(pairs >= n).any(1)] = 0
+    d_pairs = torch.from_numpy(pairs.view(np.int32).reshape(-1)).cuda()
+    d_out = torch.zeros(len(pairs), dtype=torch.uint8, device="cuda")
+    with pytest.raises(N.DvgError):
+        ctx.query_device(d, d_pairs.data_ptr(), len(pairs), d_out.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(d_out.cpu().numpy(), want)
