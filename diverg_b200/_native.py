@@ -30,7 +30,7 @@ class DvgStats(ctypes.Structure):
         "spgemm_alg_bytes", "range_ops", "h2d_bytes", "d2h_bytes", "spgemm_ns", "spgemm_levels_ns",
         "scan_ns", "spadd_ns", "spgemm_direct_tiles", "spgemm_reruns", "spgemm_light", "spgemm_slow_rows", "host_alloc_ns",
         "host_sync_ns", "spgemm_fused_adds", "graph_launches", "autotune_builds", "spgemm_levels",
-        "host_prepare_ns", "host_launch_ns", "host_meminfo_ns")]
+        "host_prepare_ns", "host_launch_ns", "host_meminfo_ns", "query_ns", "query_pairs")]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

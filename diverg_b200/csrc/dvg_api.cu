@@ -214,6 +214,7 @@ void resolve_spans(dvg_context* ctx) {
       case kProduct: ctx->stats.spgemm_ns += ns; break;
       case kLevels: ctx->stats.spgemm_levels_ns += ns; break;
       case kScan: ctx->stats.scan_ns += ns; break;
+      case kQuery: ctx->stats.query_ns += ns; break;
       default: ctx->stats.spadd_ns += ns; break;
     }
     ctx->event_pool.push_back(t.begin);
@@ -1110,7 +1111,10 @@ dvg_status dvg_query_batch(dvg_context* ctx, const dvg_matrix* index, const uint
     require(index && (npairs == 0 || (d_pairs && d_out)), "null argument");
     require((reinterpret_cast<uintptr_t>(d_pairs) & 7) == 0, "pairs must be 8-byte aligned");
     reset_control(ctx);
+    cudaEvent_t t0 = span_begin(ctx);
     launch_query(ctx, index, d_pairs, npairs, d_out);
+    span_end(ctx, t0, kQuery);
+    ctx->stats.query_pairs += npairs;
     DeviceControl c = read_control(ctx);
     if (c.invalid) throw Error(DVG_ERR_INVALID_ARG, std::to_string(c.invalid) + " query pairs out of range");
   });
@@ -1134,7 +1138,10 @@ dvg_status dvg_query_batch_host(dvg_context* ctx, const dvg_matrix* index, const
     }
     DVG_CUDA(cudaMemcpyAsync(ctx->d_pairs, pairs, npairs * 8, cudaMemcpyHostToDevice, ctx->stream));
     reset_control(ctx);
+    cudaEvent_t t0 = span_begin(ctx);
     launch_query(ctx, index, ctx->d_pairs, npairs, ctx->d_answers);
+    span_end(ctx, t0, kQuery);
+    ctx->stats.query_pairs += npairs;
     DVG_CUDA(cudaMemcpyAsync(out, ctx->d_answers, npairs, cudaMemcpyDeviceToHost, ctx->stream));
     ctx->stats.h2d_bytes += npairs * 8;
     ctx->stats.d2h_bytes += npairs;

@@ -130,7 +130,7 @@ void free_matrix(dvg_context* ctx, dvg_matrix* m);
 // Kernel timing with CUDA events on ctx->stream (active with the "timing"
 // option): span_begin records a start event, span_end its end and the kind.
 // kProduct: a single-pass SpGEMM kernel; kLevels: building union levels of B
-enum TimedKind { kProduct = 0, kLevels = 1, kScan = 2, kSpadd = 3 };
+enum TimedKind { kProduct = 0, kLevels = 1, kScan = 2, kSpadd = 3, kQuery = 4 };
 cudaEvent_t span_begin(dvg_context* ctx);
 void span_end(dvg_context* ctx, cudaEvent_t begin, TimedKind kind);
 

@@ -74,6 +74,8 @@ typedef struct dvg_stats {
   uint64_t host_prepare_ns;     /* host time planning builds (buffers, shapes) */
   uint64_t host_launch_ns;      /* host time issuing the planned builds' work */
   uint64_t host_meminfo_ns;     /* host time querying free device memory */
+  uint64_t query_ns;            /* membership-query kernels (with the "timing" option) */
+  uint64_t query_pairs;         /* locus pairs answered */
 } dvg_stats;
 
 /* ---- runtime: runtime.hpp:22-53 (initialize_runtime / finalize_runtime /
