@@ -56,7 +56,8 @@ class GraphStats(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_uint64),
-                ("max_batch_builds", ctypes.c_uint32), ("max_inflight_queries", ctypes.c_uint32)]
+                ("max_batch_builds", ctypes.c_uint32), ("max_inflight_queries", ctypes.c_uint32),
+                ("build_workers", ctypes.c_uint32)]
 
 
 class Completion(ctypes.Structure):
@@ -70,7 +71,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "builds_submitted", "builds_done", "build_batches", "queries_submitted", "queries_done", "pairs_answered",
         "resident_bytes", "peak_reserved_bytes", "hbm_budget_bytes", "build_reruns", "build_batch_ns_max",
-        "build_alloc_ns", "build_sync_ns")]
+        "build_alloc_ns", "build_sync_ns", "builds_failed", "builds_rebuilt_alone")]
 
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

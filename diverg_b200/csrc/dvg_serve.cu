@@ -1,14 +1,19 @@
 // dvg_serve.cu -- the request loop: index builds and query batches as they
 // arrive, indices resident in HBM, continuous batching.
 //
-// Two workers share one GPU, each with its own context (stream, allocator):
-//  * the build worker admits waiting builds in arrival order while their
-//    predicted footprint (predict_build_bytes: the planned build's live
-//    buffers at its estimated capacities) fits the HBM budget next to the
-//    resident indices, uploads them and builds all admitted graphs as one
-//    batch (dvg_batch.cu: one CUDA-graph launch per batch).  Builds that
-//    arrive while a batch is on the GPU join the next batch: slots free up as
-//    batches finish and indices are released;
+// Workers share one GPU, each with its own context (stream, allocator):
+//  * build_workers build workers (2 by default): a free worker admits the
+//    waiting builds in arrival order while their predicted footprint
+//    (predict_build_bytes: the planned build's live buffers at its estimated
+//    capacities) fits the HBM budget next to the resident indices and the
+//    builds in flight, uploads them and builds all admitted graphs as one
+//    batch (dvg_batch.cu: one CUDA-graph launch per batch).  A build that
+//    arrives while batches are on the GPU is taken by the next free worker at
+//    once -- its work overlaps theirs on another stream -- or, with every
+//    worker busy, joins the next batch as slots and memory free up.  Each
+//    request is checked on its own upload: a malformed graph fails alone, and
+//    if a batch fails as a whole its members are rebuilt one by one, so one
+//    bad request never fails its batch-mates;
 //  * the query worker issues every query batch whose index is resident on its
 //    own stream -- pairs in, membership kernel, answers out, an event -- with
 //    up to max_inflight_queries batches on the device at once, concurrently
@@ -57,7 +62,8 @@ struct QueryReq {
 };
 
 struct ServerIndex {
-  dvg_matrix* m = nullptr;  // allocated by the build context
+  dvg_matrix* m = nullptr;  // allocated by the build context `owner`
+  dvg_context* owner = nullptr;
   int state = 0;            // 0 building, 1 resident, -1 failed
   dvg_status error = DVG_OK;
   uint64_t bytes = 0;
@@ -86,14 +92,14 @@ struct QuerySlot {
 
 struct dvg_server {
   dvg_server_config cfg{};
-  dvg_context* bctx = nullptr;
+  std::vector<dvg_context*> bctxs;  // one per build worker
   dvg_context* qctx = nullptr;
   std::mutex mu;
   std::condition_variable cv_build, cv_query, cv_done;
   std::deque<BuildReq> builds;
   std::deque<QueryReq> queries;
   std::unordered_map<uint64_t, ServerIndex> indices;
-  std::vector<dvg_matrix*> to_free;  // released indices, freed by the build worker
+  std::vector<std::pair<dvg_context*, dvg_matrix*>> to_free;  // released indices (owner, matrix)
   std::vector<void*> retired_host;   // outgrown pinned staging, freed at shutdown
   std::deque<dvg_completion> done;
   uint64_t next_id = 1;
@@ -101,7 +107,8 @@ struct dvg_server {
   double growth = 3.0;  // the build context's capacity estimate, for admission
   dvg_server_stats st{};
   bool stop = false;
-  std::thread tb, tq;
+  std::vector<std::thread> tbs;
+  std::thread tq;
   std::vector<QuerySlot> slots;
 };
 
@@ -132,7 +139,7 @@ void maybe_drop(dvg_server* s, uint64_t id) {
   auto f = s->indices.find(id);
   if (f == s->indices.end() || !f->second.released || f->second.users) return;
   if (f->second.m) {
-    s->to_free.push_back(f->second.m);
+    s->to_free.emplace_back(f->second.owner, f->second.m);
     s->resident -= f->second.bytes;
   }
   s->indices.erase(f);
@@ -140,19 +147,30 @@ void maybe_drop(dvg_server* s, uint64_t id) {
   s->cv_build.notify_all();
 }
 
-// ---- build worker -----------------------------------------------------------
+// ---- build workers -----------------------------------------------------------
 
-void build_worker(dvg_server* s) {
+// Frees released indices, each by the context that allocated it.
+void free_released(std::vector<std::pair<dvg_context*, dvg_matrix*>>& frees) {
+  for (auto& f : frees) {
+    std::lock_guard<std::recursive_mutex> owner_lock(f.first->mu);
+    dvg::free_matrix(f.first, f.second);
+  }
+  frees.clear();
+}
+
+void build_worker(dvg_server* s, size_t w) {
+  dvg_context* ctx = s->bctxs[w];
   cudaSetDevice(s->cfg.device);
   for (;;) {
     std::vector<BuildReq> batch;
-    std::vector<dvg_matrix*> frees;
+    std::vector<std::pair<dvg_context*, dvg_matrix*>> frees;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv_build.wait(lk, [&] { return s->stop || !s->builds.empty() || !s->to_free.empty(); });
       frees.swap(s->to_free);
       if (s->stop && s->builds.empty() && frees.empty()) break;
-      uint64_t avail = s->cfg.hbm_budget_bytes > s->resident ? s->cfg.hbm_budget_bytes - s->resident : 0;
+      const uint64_t held = s->resident + s->reserved;
+      uint64_t avail = s->cfg.hbm_budget_bytes > held ? s->cfg.hbm_budget_bytes - held : 0;
       while (!s->builds.empty() && batch.size() < s->cfg.max_batch_builds) {
         BuildReq& r = s->builds.front();
         if (r.predicted > avail) {
@@ -172,7 +190,7 @@ void build_worker(dvg_server* s) {
             s->cv_query.notify_all();
             continue;
           }
-          break;  // waits until released indices free memory
+          break;  // waits until builds in flight finish or released indices free memory
         }
         avail -= r.predicted;
         s->reserved += r.predicted;
@@ -186,38 +204,79 @@ void build_worker(dvg_server* s) {
       }
     }
     // ---- GPU work, outside the server lock ----------------------------------
-    std::lock_guard<std::recursive_mutex> ctx_lock(s->bctx->mu);
-    for (dvg_matrix* m : frees) dvg::free_matrix(s->bctx, m);
+    free_released(frees);
     if (batch.empty()) continue;
+    std::lock_guard<std::recursive_mutex> ctx_lock(ctx->mu);
     const uint64_t t_start = now();
-    std::vector<dvg_matrix*> in(batch.size(), nullptr), out(batch.size(), nullptr);
-    std::vector<unsigned> lo(batch.size()), hi(batch.size());
-    dvg_status status = DVG_OK;
-    try {
-      for (size_t k = 0; k < batch.size(); ++k) {
-        in[k] = dvg::upload_matrix(s->bctx, batch[k].n, batch[k].n, batch[k].rowmap, batch[k].entries, 0);
-        lo[k] = batch[k].dmin;
-        hi[k] = batch[k].dmax;
+    const size_t nb = batch.size();
+    std::vector<dvg_matrix*> in(nb, nullptr), out(nb, nullptr);
+    std::vector<dvg_status> status(nb, DVG_OK);
+    std::vector<std::string> why(nb);
+    // every request's upload checked on its own: a malformed graph fails alone
+    std::vector<size_t> ok;
+    for (size_t k = 0; k < nb; ++k) {
+      try {
+        in[k] = dvg::upload_matrix(ctx, batch[k].n, batch[k].n, batch[k].rowmap, batch[k].entries, 0);
+        ok.push_back(k);
+      } catch (const Error& e) {
+        status[k] = e.status;
+        why[k] = e.what();
+      } catch (const std::exception& e) {
+        status[k] = DVG_ERR_DEVICE;
+        why[k] = e.what();
       }
-      dvg::batch_distance_index(s->bctx, uint32_t(batch.size()), in.data(), lo.data(), hi.data(), out.data());
-    } catch (const Error& e) {
-      status = e.status;
-      dvg::record_error(e.what());
-    } catch (const std::exception& e) {
-      status = DVG_ERR_DEVICE;
-      dvg::record_error(e.what());
     }
-    for (dvg_matrix* m : in) dvg::free_matrix(s->bctx, m);
+    auto build = [&](const std::vector<size_t>& members) {
+      std::vector<dvg_matrix*> gi, go(members.size(), nullptr);
+      std::vector<unsigned> lo, hi;
+      for (size_t k : members) {
+        gi.push_back(in[k]);
+        lo.push_back(batch[k].dmin);
+        hi.push_back(batch[k].dmax);
+      }
+      dvg::batch_distance_index(ctx, uint32_t(members.size()), gi.data(), lo.data(), hi.data(), go.data());
+      for (size_t q = 0; q < members.size(); ++q) out[members[q]] = go[q];
+    };
+    size_t reruns = 0;
+    if (!ok.empty()) {
+      try {
+        build(ok);
+      } catch (const std::exception&) {
+        // the batch failed as a whole: its members one by one, so a request
+        // that cannot build fails alone
+        for (size_t k : ok) {
+          ++reruns;
+          try {
+            build(std::vector<size_t>{k});
+          } catch (const Error& e) {
+            status[k] = e.status;
+            why[k] = e.what();
+          } catch (const std::exception& e) {
+            status[k] = DVG_ERR_DEVICE;
+            why[k] = e.what();
+          }
+        }
+      }
+    }
+    for (dvg_matrix* m : in)
+      if (m) dvg::free_matrix(ctx, m);
     const uint64_t t_done = now();
     {
       std::lock_guard<std::mutex> lk(s->mu);
-      s->growth = s->bctx->plan_growth;
+      s->growth = std::max(s->growth, ctx->plan_growth);
       s->st.build_batches++;
-      s->st.build_reruns = s->bctx->stats.spgemm_reruns;
+      s->st.builds_rebuilt_alone += reruns;
       s->st.build_batch_ns_max = std::max(s->st.build_batch_ns_max, t_done - t_start);
-      s->st.build_alloc_ns = s->bctx->stats.host_alloc_ns;
-      s->st.build_sync_ns = s->bctx->stats.host_sync_ns;
-      for (size_t k = 0; k < batch.size(); ++k) {
+      uint64_t alloc_ns = 0, sync_ns = 0, cap_reruns = 0;
+      for (dvg_context* c : s->bctxs) {
+        alloc_ns += c->stats.host_alloc_ns;
+        sync_ns += c->stats.host_sync_ns;
+        cap_reruns += c->stats.spgemm_reruns;
+      }
+      s->st.build_alloc_ns = alloc_ns;
+      s->st.build_sync_ns = sync_ns;
+      s->st.build_reruns = cap_reruns;
+      for (size_t k = 0; k < nb; ++k) {
         ServerIndex& ix = s->indices[batch[k].id];
         s->reserved -= batch[k].predicted;
         dvg_completion c{};
@@ -226,8 +285,9 @@ void build_worker(dvg_server* s) {
         c.submit_ns = batch[k].submit_ns;
         c.start_ns = t_start;
         c.done_ns = t_done;
-        if (status == DVG_OK) {
+        if (status[k] == DVG_OK && out[k]) {
           ix.m = out[k];
+          ix.owner = ctx;
           ix.state = 1;
           ix.bytes = dvg::matrix_bytes(out[k]);
           s->resident += ix.bytes;
@@ -237,14 +297,17 @@ void build_worker(dvg_server* s) {
           s->st.builds_done++;
         } else {
           ix.state = -1;
-          ix.error = status;
-          c.status = status;
+          ix.error = status[k] == DVG_OK ? DVG_ERR_DEVICE : status[k];
+          c.status = ix.error;
+          s->st.builds_failed++;
+          if (!why[k].empty()) dvg::record_error(why[k]);
         }
         complete(s, c);
       }
       s->st.resident_bytes = s->resident;
     }
     s->cv_query.notify_all();
+    s->cv_build.notify_all();  // reserved memory came back: another worker may admit now
   }
 }
 
@@ -425,7 +488,13 @@ dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out) {
   s->cfg = *cfg;
   if (!s->cfg.max_batch_builds) s->cfg.max_batch_builds = 64;
   if (!s->cfg.max_inflight_queries) s->cfg.max_inflight_queries = 8;
-  dvg_status st = dvg_init(cfg->device, &s->bctx);
+  if (!s->cfg.build_workers) s->cfg.build_workers = 2;
+  dvg_status st = DVG_OK;
+  for (uint32_t w = 0; w < s->cfg.build_workers && st == DVG_OK; ++w) {
+    dvg_context* c = nullptr;
+    st = dvg_init(cfg->device, &c);
+    if (st == DVG_OK) s->bctxs.push_back(c);
+  }
   if (st == DVG_OK) st = dvg_init(cfg->device, &s->qctx);
   if (st == DVG_OK) {
     try {
@@ -451,9 +520,9 @@ dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out) {
       {
         const uint64_t warm = std::min<uint64_t>(s->cfg.hbm_budget_bytes, uint64_t(8) << 30);
         void* p = nullptr;
-        if (cudaMallocAsync(&p, warm, s->bctx->stream) == cudaSuccess) {
-          DVG_CUDA(cudaFreeAsync(p, s->bctx->stream));
-          DVG_CUDA(cudaStreamSynchronize(s->bctx->stream));
+        if (cudaMallocAsync(&p, warm, s->bctxs[0]->stream) == cudaSuccess) {
+          DVG_CUDA(cudaFreeAsync(p, s->bctxs[0]->stream));
+          DVG_CUDA(cudaStreamSynchronize(s->bctxs[0]->stream));
         } else {
           (void)cudaGetLastError();
         }
@@ -464,9 +533,9 @@ dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out) {
         DVG_CUDA(cudaMallocHost(&q.h_ctl, sizeof(DeviceControl)));
         DVG_CUDA(cudaEventCreateWithFlags(&q.done, cudaEventDisableTiming));
       }
-      s->growth = s->bctx->plan_growth;
+      s->growth = s->bctxs[0]->plan_growth;
       // batches in a request stream vary in size: no timing runs on the way
-      s->bctx->opt_autotune = 0;
+      for (dvg_context* c : s->bctxs) c->opt_autotune = 0;
       s->st.hbm_budget_bytes = s->cfg.hbm_budget_bytes;
     } catch (const Error& e) {
       dvg::record_error(e.what());
@@ -479,11 +548,11 @@ dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out) {
       if (q.done) cudaEventDestroy(q.done);
     }
     if (s->qctx) dvg_shutdown(s->qctx);
-    if (s->bctx) dvg_shutdown(s->bctx);
+    for (dvg_context* c : s->bctxs) dvg_shutdown(c);
     delete s;
     return st;
   }
-  s->tb = std::thread(build_worker, s);
+  for (size_t w = 0; w < s->bctxs.size(); ++w) s->tbs.emplace_back(build_worker, s, w);
   s->tq = std::thread(query_worker, s);
   *out = s;
   return DVG_OK;
@@ -497,11 +566,11 @@ dvg_status dvg_server_destroy(dvg_server* s) {
   }
   s->cv_build.notify_all();
   s->cv_query.notify_all();
-  s->tb.join();
+  for (auto& t : s->tbs) t.join();
   s->tq.join();
   for (auto& kv : s->indices)
-    if (kv.second.m) dvg::free_matrix(s->bctx, kv.second.m);
-  for (dvg_matrix* m : s->to_free) dvg::free_matrix(s->bctx, m);
+    if (kv.second.m) dvg::free_matrix(kv.second.owner, kv.second.m);
+  free_released(s->to_free);
   for (auto& q : s->slots) {
     if (q.h_pairs) cudaFreeHost(q.h_pairs);
     if (q.h_out) cudaFreeHost(q.h_out);
@@ -509,7 +578,11 @@ dvg_status dvg_server_destroy(dvg_server* s) {
     if (q.done) cudaEventDestroy(q.done);
   }
   for (void* h : s->retired_host) cudaFreeHost(h);
-  dvg_status a = dvg_shutdown(s->qctx), b = dvg_shutdown(s->bctx);
+  dvg_status a = dvg_shutdown(s->qctx), b = DVG_OK;
+  for (dvg_context* c : s->bctxs) {
+    const dvg_status x = dvg_shutdown(c);
+    if (b == DVG_OK) b = x;
+  }
   delete s;
   return a != DVG_OK ? a : b;
 }

@@ -22,8 +22,9 @@ class Server:
     """A dvg_server on one device.  Arrays handed to a request are kept alive
     here until its completion has been polled."""
 
-    def __init__(self, device=0, hbm_budget_bytes=0, max_batch_builds=0, max_inflight_queries=0):
-        cfg = N.ServerConfig(device, int(hbm_budget_bytes), int(max_batch_builds), int(max_inflight_queries))
+    def __init__(self, device=0, hbm_budget_bytes=0, max_batch_builds=0, max_inflight_queries=0, build_workers=0):
+        cfg = N.ServerConfig(device, int(hbm_budget_bytes), int(max_batch_builds), int(max_inflight_queries),
+                             int(build_workers))
         h = ctypes.c_void_p()
         N.check(N.lib().dvg_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -126,6 +127,7 @@ def run_stream(server, graphs, pair_pool, answer_pool, rate, nreq, seed, window=
     drawn earlier build.  Returns latencies (ms) per kind and the throughput."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, nreq)
+    gaps *= (nreq / rate) / gaps.sum()  # the stream's mean rate is the nominal one
     kinds = rng.random(nreq) < 0.2
     sizes = rng.integers(100_000, 1_000_001, nreq)
     built = []          # (build id, graph index)
@@ -180,8 +182,8 @@ def run_stream(server, graphs, pair_pool, answer_pool, rate, nreq, seed, window=
         first_submit = c["submit_ns"] if first_submit is None else min(first_submit, c["submit_ns"])
         last_submit = c["submit_ns"] if last_submit is None else max(last_submit, c["submit_ns"])
     span_s = (last_done - first_submit) / 1e9
-    # the rate actually offered: the Poisson gaps of a finite stream, and the
-    # submitting loop itself, make it differ from the nominal rate
+    # the rate actually offered: the submitting loop can fall behind the
+    # arrival times
     offered = (nreq - 1) / max((last_submit - first_submit) / 1e9, 1e-9)
     return {"rate": rate, "offered": offered, "requests": nreq, "failed": failed, "throughput": nreq / span_s,
             "wall_s": t_end - t0, "build_latency_ms": _percentiles(lat[BUILD]),
@@ -203,7 +205,7 @@ def bench_line(args, ctx, rank, requests=None, max_rate=51200.0):
     fixed rate the sweep doubles the arrival rate from 200/s until the served
     throughput falls below 95 % of the offered rate (or a request fails): the
     knee is the highest rate still served at >= 95 % of the rate actually
-    offered (a finite Poisson stream's span varies), and the first rate past
+    offered (the submitting loop can fall behind), and the first rate past
     it is reported beside it."""
     import torch
     from . import gen

@@ -278,6 +278,7 @@ typedef struct dvg_server_config {
   uint64_t hbm_budget_bytes;     /* resident indices + builds in flight; 0: 80 % of free memory */
   uint32_t max_batch_builds;     /* builds merged into one batch; 0: 64 */
   uint32_t max_inflight_queries; /* query batches on the device at once; 0: 8 */
+  uint32_t build_workers;        /* build batches on the device at once, each on its own stream; 0: 2 */
 } dvg_server_config;
 
 typedef struct dvg_completion {
@@ -305,7 +306,9 @@ typedef struct dvg_server_stats {
   uint64_t build_reruns;         /* builds whose planned capacity was outgrown: re-run step by step */
   uint64_t build_batch_ns_max;   /* longest build batch, host clock */
   uint64_t build_alloc_ns;       /* build worker: host time in device allocation calls */
-  uint64_t build_sync_ns;        /* build worker: host time waiting for its stream */
+  uint64_t build_sync_ns;        /* build workers: host time waiting for their streams */
+  uint64_t builds_failed;        /* builds completed with an error (each alone: batch-mates unaffected) */
+  uint64_t builds_rebuilt_alone; /* members of a failed batch built again one by one */
 } dvg_server_stats;
 
 dvg_status dvg_server_create(const dvg_server_config* cfg, dvg_server** out);

@@ -109,3 +109,55 @@ def test_oversized_builds_bad_pairs_and_released_indices_report_errors():
         assert c["status"] == N.INVALID_ARG
         with pytest.raises(N.DvgError):
             srv.release(b)
+
+
+def _malformed(g, kind):
+    """g with one defect the upload check rejects: an odd row length, or a
+    column past the last one."""
+    rowmap = g.rowmap.astype(np.uint64).copy()
+    entries = g.entries.copy()
+    if kind == "odd_row":
+        rowmap[1:] += 1  # row 0 one entry longer: an odd count
+        entries = np.concatenate([entries[:1], entries]).astype(np.uint32)
+    else:
+        entries[-1] = g.numCols()
+    return CRSMatrix(g.numCols(), entries, rowmap, 1)
+
+
+@pytest.mark.parametrize("kind", ["odd_row", "column"])
+def test_a_malformed_build_fails_alone(kind):
+    # one worker, a long build first: the rest queue and go out as one batch
+    # with the malformed graph among them; it fails with INVALID_ARG, its
+    # batch-mates build and match the oracle
+    first = graph(400_000, seed=500)
+    mates = [graph(8_000 + 1_000 * k, seed=501 + k) for k in range(5)]
+    bad = _malformed(graph(6_000, seed=510), kind)
+    with Server(device=0, max_batch_builds=16, build_workers=1) as srv:
+        b0 = srv.submit_build(first, *WINDOW)
+        ids = [srv.submit_build(m, *WINDOW) for m in mates[:2]]
+        bid = srv.submit_build(bad, *WINDOW)
+        ids += [srv.submit_build(m, *WINDOW) for m in mates[2:]]
+        done = {c["request"]: c for c in srv.wait([b0, bid] + ids)}
+        assert done[bid]["status"] == N.INVALID_ARG
+        assert all(done[i]["status"] == N.OK for i in [b0] + ids)
+        for k, i in enumerate(ids):
+            want = orc.dindex(omat(mates[k]), *WINDOW, algo="hbv")
+            assert same(srv.download(i), CRSMatrix(want.ncols, want.entries, want.rowmap, want.nnz)), k
+        st = srv.stats()
+        assert st["builds_failed"] == 1 and st["builds_done"] == 6
+
+
+def test_builds_run_side_by_side_on_two_workers():
+    # a long build holds one worker; a short build submitted after it is
+    # taken by the other worker and completes first, and both are right
+    long_g = graph(2_000_000, seed=520)
+    short_g = graph(5_000, seed=521)
+    with Server(device=0, max_batch_builds=1, build_workers=2) as srv:
+        bl = srv.submit_build(long_g, *WINDOW)
+        bs = srv.submit_build(short_g, *WINDOW)
+        cl, cs = srv.wait([bl, bs])
+        assert cl["status"] == N.OK and cs["status"] == N.OK
+        assert cs["done_ns"] < cl["done_ns"]
+        for g, b in ((long_g, bl), (short_g, bs)):
+            want = orc.dindex(omat(g), *WINDOW, algo="hbv")
+            assert same(srv.download(b), CRSMatrix(want.ncols, want.entries, want.rowmap, want.nnz))
