@@ -39,6 +39,10 @@ constexpr int kRowRowsMax = kChunkMax / kThreads;  // rows per thread at the lar
 constexpr int kRowDirectWW = 192;  // warp path: 32-bit window words per warp (6,144 columns)
 constexpr int kAStage = 2048;      // A ranges of a chunk staged in shared memory
 constexpr int kRowStagePerRow = 16;  // staged entries per chunk row (a chunk with more is written in place)
+// general-walk list entries: the chunk row, and whether it went on to the
+// warp path or (past kSlowMax of those) to the light path
+constexpr uint32_t kGenRow = 0x0fffu, kGenWarp = 0x4000u, kGenLight = 0x8000u;
+static_assert(kChunkMax <= int(kGenRow) + 1, "chunk rows must fit the general-walk list entries");
 
 // The chunk's A row pointers and (up to kAStage of) its A ranges, loaded with
 // coalesced reads before the rows are walked; the warp path's windows reuse
@@ -61,6 +65,7 @@ struct RowSmem {
   RowScratch u;
   uint32_t incl[kChunkMax];             // the counted chunk's (then chunk-local inclusive) row counts
   uint32_t slow[kSlowMax];              // rows of the counted chunk left to the warp path
+  uint16_t gen[kChunkMax];              // rows left to the general walk (| kGenWarp, kGenLight: how it ended)
   unsigned long long red[kWarps];
   unsigned long long red_nnz[kWarps];
   unsigned long long lb_sum[2][kWarps];  // look-back records by round parity, per warp
@@ -74,6 +79,7 @@ struct RowSmem {
   uint32_t pend_t[2], pend_crows[2];
   uint32_t next;                        // the chunk taken for the next iteration
   uint32_t nslow;
+  uint32_t ngen;
 };
 
 // Accumulates chunk row r (C row `row`) into the thread's slot from entry
@@ -208,6 +214,40 @@ __device__ bool row_runs(RowSmem<SLOT>& S, const FusedArgs& p, uint64_t row, uin
   return true;
 }
 
+// The union of at most two ranges (an empty one has y < x) into the slot at
+// `pos`: one run, or two when they neither overlap nor touch.  Columns are
+// below 2^32 - 2, so hi + 1 does not wrap.  False when the runs do not fit.
+template <int SLOT>
+__device__ __forceinline__ bool two_ranges(RowSmem<SLOT>& S, uint2 x, uint2 y, uint32_t pos, uint32_t& count,
+                                           unsigned long long& nnz) {
+  if (x.y < x.x) x = y;
+  if (y.y < y.x) y = x;
+  if (y.x < x.x) {
+    const uint2 s = x;
+    x = y;
+    y = s;
+  }
+  uint32_t nr = 0;
+  if (x.x <= x.y) nr = y.x <= x.y + 1 ? 1u : 2u;
+  if (nr > (uint32_t(SLOT) - pos) >> 1) return false;
+  uint32_t* L = S.slot + threadIdx.x + size_t(pos) * kThreads;
+  uint64_t n = 0;
+  if (nr == 1) x.y = max(x.y, y.y);
+  if (nr) {
+    L[0] = x.x;
+    L[kThreads] = x.y;
+    n = uint64_t(x.y) - x.x + 1;
+  }
+  if (nr == 2) {
+    L[2 * kThreads] = y.x;
+    L[3 * kThreads] = y.y;
+    n += uint64_t(y.y) - y.x + 1;
+  }
+  count = 2 * nr;
+  nnz += n;
+  return true;
+}
+
 // The row kernel.  With rpt = ceil(chunk_rows / kThreads) rows per thread,
 // thread (warp, lane) owns chunk rows (warp * rpt + u) * 32 + lane, u < rpt:
 // the lanes of a warp take consecutive rows.
@@ -242,6 +282,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   if (tid == 0) {
     S.next = take_ticket();
     S.nslow = 0;
+    S.ngen = 0;
   }
   cta_sync();
   uint32_t t = S.next, b = 0, par = 0;
@@ -250,6 +291,64 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
   // the asynchronous stage copies 8-byte words
   const bool a_async = !A_ID && ((reinterpret_cast<uintptr_t>(p.a_rowmap) | reinterpret_cast<uintptr_t>(p.a_entries)) & 7u) == 0;
   uint32_t iter = 0;
+  // Writes the counted chunk's rows at out + their chunk-local offsets, where
+  // `room` entries fit: the common rows from their owners' slots, the general
+  // rows from their walkers' slots (light-path rows recomputed by their
+  // walkers), the warp-path rows recomputed by the warps.  Rows past `room`
+  // are skipped (and, with flag, reported as an overflow).
+  auto write_rows = [&](uint32_t* out, unsigned long long room, bool flag, uint32_t c0row, uint32_t crows,
+                        uint32_t fast_mask, uint32_t ngen, uint32_t nslow) {
+    const uint32_t* incl = S.incl;
+    uint32_t spos = 0;
+#pragma unroll 1
+    for (int u = 0; u < kRowRowsMax; ++u) {
+      if (uint32_t(u) >= rpt) break;
+      const uint32_t r = (warp * rpt + u) * 32 + lane;
+      if (r >= crows || !((fast_mask >> u) & 1u)) continue;
+      const uint32_t o = r ? incl[r - 1] : 0u;
+      const uint32_t n = incl[r] - o;
+      if (uint64_t(o) + n <= room) {
+        for (uint32_t k = 0; k < n; ++k) out[o + k] = S.slot[(spos + k) * kThreads + tid];
+      } else if (flag && n) {
+        raise_flag(p, &p.ctl->overflow, 1ull);
+      }
+      spos += n;
+    }
+    for (uint32_t i = uint32_t(lane) * kWarps + warp; i < ngen; i += kThreads) {
+      const uint32_t e = S.gen[i], r = e & kGenRow;
+      if (e & kGenWarp) continue;
+      const uint32_t o = r ? incl[r - 1] : 0u;
+      const uint32_t n = incl[r] - o;
+      if (uint64_t(o) + n > room) {
+        if (flag && n) raise_flag(p, &p.ctl->overflow, 1ull);
+      } else if (e & kGenLight) {
+        uint32_t* dst = out + o;
+        const uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
+                                           [&](uint64_t k, uint32_t v) {
+                                             if (k < n) dst[k] = v;
+                                           });
+        if (c != n) raise_flag(p, &p.ctl->status, 8ull);
+      } else {
+        for (uint32_t k = 0; k < n; ++k) out[o + k] = S.slot[(spos + k) * kThreads + tid];
+      }
+      if (!(e & kGenLight)) spos += n;
+    }
+    for (uint32_t i = warp; i < nslow; i += kWarps) {
+      const uint32_t r = S.slow[i];
+      const uint32_t o = r ? incl[r - 1] : 0u;
+      const uint32_t n = incl[r] - o;
+      if (n == 0 || uint64_t(o) + n > room) continue;
+      uint32_t* dst = out + o;
+      bool bad = false;
+      const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
+                                    [&](uint64_t k, uint32_t v) {
+                                      if (k < n) dst[k] = v;
+                                      else bad = true;
+                                    },
+                                    kRowDirectWW);
+      if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+    }
+  };
   while (t < p.nchunks || pend) {
     const bool have = t < p.nchunks;
     // thread 0 takes the next ticket while the rows are walked (its latency
@@ -260,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     const uint32_t crows = have ? min(p.chunk_rows, p.nrows - c0row) : 0u;
     uint32_t* const incl = S.incl;
     unsigned long long nnz_acc = 0, cnt = 0, cnnz = 0;
-    uint32_t fast_mask = 0, nslow = 0, nslow_all = 0;
+    uint32_t fast_mask = 0, nslow = 0, ngen = 0;
     bool staged = false;
     if (have) {
       // stage A's row pointers and ranges of the chunk (coalesced)
@@ -283,42 +382,106 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
           cta_sync();
         }
       }
-      uint32_t pos = 0;
-      // rows that miss the slot wait for the warp-cooperative pass below, so
-      // one wide row never holds a whole chunk behind a single thread
-#pragma unroll 1
-      for (int u = 0; u < kRowRowsMax; ++u) {
-        if (uint32_t(u) >= rpt) break;
-        const uint32_t r = (warp * rpt + u) * 32 + lane;
-        if (r < crows) {
-          uint32_t c = 0;
-          if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, r, abase, nst, pos, c, nnz_acc)) {
-            fast_mask |= 1u << u;
-            pos += c;
+      // Rows of the common shape -- one A range whose B rows hold at most one
+      // range, an addend row of at most one range -- are counted from loads
+      // issued for all of the thread's rows at once: two dependent trips to
+      // memory for all of them, where a walk takes two or three per row.
+      uint32_t quick = 0;
+      uint2 qx[kRowRowsMax], qy[kRowRowsMax];
+      {
+        uint64_t t0[kRowRowsMax], t1[kRowRowsMax], d0[kRowRowsMax], d1[kRowRowsMax];
+        uint32_t one = 0;  // rows with one A range, staged and not read through levels
+#pragma unroll
+        for (int u = 0; u < kRowRowsMax; ++u) {
+          t0[u] = t1[u] = d0[u] = d1[u] = 0;
+          const uint32_t r = (warp * rpt + u) * 32 + lane;
+          if (uint32_t(u) >= rpt || r >= crows) continue;
+          uint2 ar = make_uint2(1u, 0u);
+          bool single = true;
+          if (A_ID) {
+            ar = id_range(p, uint64_t(c0row) + r);
           } else {
-            const uint32_t i = atomicAdd(&S.nslow, 1u);
-            if (i < uint32_t(kSlowMax)) {
-              S.slow[i] = r;
-            } else {
-              c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
-            }
-            atomicAdd(&p.ctl->slow_rows, 1ull);
+            const uint64_t a0 = S.u.a.arow[r] >> 1, a1 = S.u.a.arow[r + 1] >> 1;
+            single = a1 - a0 == 1 && a0 - abase < nst;
+            if (single) ar = S.u.a.aent[a0 - abase];
           }
-          incl[r] = c;
+          if (!single || (ar.x <= ar.y && p.nlevels && ar.y - ar.x >= 3u)) continue;
+          one |= 1u << u;
+          if (ar.x <= ar.y) {
+            t0[u] = __ldg(p.b_rowmap + ar.x);
+            t1[u] = __ldg(p.b_rowmap + uint64_t(ar.y) + 1);
+          }
+          if (p.d_rowmap) {
+            d0[u] = __ldg(p.d_rowmap + uint64_t(c0row) + r);
+            d1[u] = __ldg(p.d_rowmap + uint64_t(c0row) + r + 1);
+          }
         }
+#pragma unroll
+        for (int u = 0; u < kRowRowsMax; ++u) {
+          const uint64_t b0 = t0[u] >> 1, b1 = t1[u] >> 1, e0 = d0[u] >> 1, e1 = d1[u] >> 1;
+          qx[u] = qy[u] = make_uint2(1u, 0u);
+          if (!((one >> u) & 1u) || b1 - b0 > 1 || e1 - e0 > 1) continue;
+          quick |= 1u << u;
+          if (b1 > b0) qx[u] = load_range(p.b_entries, b0);
+          if (e1 > e0) qy[u] = load_range(p.d_entries, e0);
+        }
+      }
+      // the common rows into the thread's slot, in row order; the others are
+      // listed for the general walk, so that a warp whose lanes hold a few
+      // of them does not make the other lanes wait through it
+      uint32_t pos = 0;
+#pragma unroll
+      for (int u = 0; u < kRowRowsMax; ++u) {
+        const uint32_t r = (warp * rpt + u) * 32 + lane;
+        if (uint32_t(u) >= rpt || r >= crows) continue;
+        uint32_t c = 0;
+        const uint2 qd = p.d_identity ? make_uint2(c0row + r, c0row + r) : qy[u];
+        if (((quick >> u) & 1u) && two_ranges<SLOT>(S, qx[u], qd, pos, c, nnz_acc)) {
+          fast_mask |= 1u << u;
+          pos += c;
+          incl[r] = c;
+        } else {
+          S.gen[atomicAdd(&S.ngen, 1u)] = uint16_t(r);
+        }
+      }
+      cta_sync();
+      // the general walk, entry i by lane i / kWarps of warp i % kWarps: the
+      // warps share a chunk's few general rows; each row's runs go to the
+      // walker's slot after its own rows.  Rows that miss the slot wait for
+      // the warp-cooperative pass below, so one wide row never holds a whole
+      // chunk behind a single thread.
+      ngen = S.ngen;
+      for (uint32_t i = uint32_t(lane) * kWarps + warp; i < ngen; i += kThreads) {
+        const uint32_t r = S.gen[i];
+        uint32_t c = 0;
+        if (row_runs<A_ID, SLOT>(S, p, uint64_t(c0row) + r, r, abase, nst, pos, c, nnz_acc)) {
+          pos += c;
+        } else {
+          const uint32_t j = atomicAdd(&S.nslow, 1u);
+          if (j < uint32_t(kSlowMax)) {
+            S.slow[j] = r;
+            S.gen[i] = uint16_t(r | kGenWarp);
+          } else {
+            c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, &nnz_acc, [](uint64_t, uint32_t) {});
+            S.gen[i] = uint16_t(r | kGenLight);
+          }
+          atomicAdd(&p.ctl->slow_rows, 1ull);
+        }
+        incl[r] = c;
       }
       cta_sync();
       if (tid == 0 && !stop) next = atomicAdd(p.ticket, 1u);
       // the stage is dead from here on: the warp path may use the space
-      nslow_all = S.nslow;
-      nslow = min(nslow_all, uint32_t(kSlowMax));
-      for (uint32_t i = warp; i < nslow; i += kWarps) {
-        const uint32_t r = S.slow[i];
-        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
-                                      [](uint64_t, uint32_t) {}, kRowDirectWW);
-        if (lane == 0) incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+      nslow = min(S.nslow, uint32_t(kSlowMax));
+      if (nslow) {
+        for (uint32_t i = warp; i < nslow; i += kWarps) {
+          const uint32_t r = S.slow[i];
+          const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, &nnz_acc,
+                                        [](uint64_t, uint32_t) {}, kRowDirectWW);
+          if (lane == 0) incl[r] = uint32_t(min(c, uint64_t(0xffffffffu)));
+        }
+        cta_sync();
       }
-      cta_sync();
       // chunk prefix over the row counts (kRowRowsMax consecutive rows per
       // thread: a thread rewrites only its own rows) and the chunk's nnz
       {
@@ -362,50 +525,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
         uint32_t* img = stage + size_t(b) * (p.stage_cap + p.chunk_rows);
         if (tid == 0) publish_aggregate(p, t, cnt);
         for (uint32_t r = tid; r < crows; r += kThreads) img[p.stage_cap + r] = incl[r];
-        uint32_t spos = 0;
-#pragma unroll 1
-        for (int u = 0; u < kRowRowsMax; ++u) {
-          if (uint32_t(u) >= rpt) break;
-          const uint32_t r = (warp * rpt + u) * 32 + lane;
-          if (r >= crows || !((fast_mask >> u) & 1u)) continue;
-          const uint32_t o = r ? incl[r - 1] : 0u;
-          const uint32_t n = incl[r] - o;
-          for (uint32_t k = 0; k < n; ++k) img[o + k] = S.slot[(spos + k) * kThreads + tid];
-          spos += n;
-        }
-        for (uint32_t i = warp; i < nslow; i += kWarps) {
-          const uint32_t r = S.slow[i];
-          const uint32_t o = r ? incl[r - 1] : 0u;
-          const uint32_t n = incl[r] - o;
-          if (n == 0) continue;
-          bool bad = false;
-          const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
-                                        [&](uint64_t k, uint32_t v) {
-                                          if (k < n) img[o + k] = v;
-                                          else bad = true;
-                                        },
-                                        kRowDirectWW);
-          if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
-        }
-        if (nslow_all > uint32_t(kSlowMax)) {
-#pragma unroll 1
-          for (int u = 0; u < kRowRowsMax; ++u) {
-            if (uint32_t(u) >= rpt) break;
-            const uint32_t r = (warp * rpt + u) * 32 + lane;
-            if (r >= crows || ((fast_mask >> u) & 1u)) continue;
-            bool listed = false;
-            for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
-            if (listed) continue;
-            const uint32_t o = r ? incl[r - 1] : 0u;
-            const uint32_t n = incl[r] - o;
-            if (n == 0) continue;
-            const uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
-                                               [&](uint64_t k, uint32_t v) {
-                                                 if (k < n) img[o + k] = v;
-                                               });
-            if (c != n) raise_flag(p, &p.ctl->status, 8ull);
-          }
-        }
+        write_rows(img, ~0ull, false, c0row, crows, fast_mask, ngen, nslow);
       }
     }
     if (tid == 0) S.next = next;
@@ -483,57 +603,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       const unsigned long long prefix = lookback_block(S, p, t, cnt, par);
       for (uint32_t r = tid; r < crows; r += kThreads) p.c_rowmap[uint64_t(c0row) + r + 1] = prefix + incl[r];
       if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
-      uint32_t pos = 0;
-#pragma unroll 1
-      for (int u = 0; u < kRowRowsMax; ++u) {
-        if (uint32_t(u) >= rpt) break;
-        const uint32_t r = (warp * rpt + u) * 32 + lane;
-        if (r >= crows) continue;
-        const unsigned long long dst = prefix + (r ? incl[r - 1] : 0u);
-        const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
-        const bool fast = (fast_mask >> u) & 1u;
-        if (n && dst + n > p.cap) {
-          raise_flag(p, &p.ctl->overflow, 1ull);
-        } else if (fast) {
-          for (uint32_t k = 0; k < n; ++k) p.c_entries[dst + k] = S.slot[(pos + k) * kThreads + tid];
-        }
-        if (fast) pos += n;
-      }
-      for (uint32_t i = warp; i < nslow; i += kWarps) {
-        const uint32_t r = S.slow[i];
-        const unsigned long long dst = prefix + (r ? incl[r - 1] : 0u);
-        const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
-        if (n == 0 || dst + n > p.cap) continue;
-        uint32_t* out = p.c_entries + dst;
-        bool bad = false;
-        const uint64_t c = direct_row(p, A_ID, uint64_t(c0row) + r, dbits, dreach, nullptr,
-                                      [&](uint64_t k, uint32_t v) {
-                                        if (k < n) out[k] = v;
-                                        else bad = true;
-                                      },
-                                      kRowDirectWW);
-        if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
-      }
-      if (nslow_all > uint32_t(kSlowMax)) {
-#pragma unroll 1
-        for (int u = 0; u < kRowRowsMax; ++u) {
-          if (uint32_t(u) >= rpt) break;
-          const uint32_t r = (warp * rpt + u) * 32 + lane;
-          if (r >= crows || ((fast_mask >> u) & 1u)) continue;
-          bool listed = false;
-          for (uint32_t i = 0; i < nslow && !listed; ++i) listed = S.slow[i] == r;
-          if (listed) continue;
-          const unsigned long long dst = prefix + (r ? incl[r - 1] : 0u);
-          const uint32_t n = incl[r] - (r ? incl[r - 1] : 0u);
-          if (n == 0 || dst + n > p.cap) continue;
-          uint32_t* out = p.c_entries + dst;
-          uint32_t c = light_row<A_ID>(nullptr, nullptr, p, c0row, r, false, nullptr,
-                                       [&](uint64_t k, uint32_t v) {
-                                         if (k < n) out[k] = v;
-                                       });
-          if (c != n) raise_flag(p, &p.ctl->status, 8ull);
-        }
-      }
+      write_rows(p.c_entries + prefix, p.cap > prefix ? p.cap - prefix : 0ull, true, c0row, crows, fast_mask, ngen,
+                 nslow);
     }
     if (tid == 0 && staged) {  // the image just written, in buffer b
       S.pend_t[b] = t;
@@ -547,7 +618,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     // the next chunk; every warp must have passed the same barriers
     ++iter;
     if (lane == 0) S.phase[warp] = iter;
-    if (tid == 0) S.nslow = 0;
+    if (tid == 0) {
+      S.nslow = 0;
+      S.ngen = 0;
+    }
     cta_sync();
     if (warp == 0) {  // one read per lane, one vote
       const bool off = lane < kWarps && S.phase[lane] != iter;
