@@ -362,9 +362,28 @@ __device__ __forceinline__ void publish_aggregate(const FusedArgs& p, uint32_t t
 // alternate between two sets by round (`par` runs on across calls), so a
 // round's writes never meet the previous round's reads.  Waits are bounded;
 // every branch is uniform over the CTA.
+// The descriptor a thread reads in the first round of chunk t's look-back,
+// read ahead of it (a descriptor only ever moves on from nothing to an
+// aggregate to an inclusive prefix, so an early read is an earlier state).
+struct LookbackAhead {
+  unsigned long long agg, incl;
+  bool valid;
+};
+__device__ __forceinline__ LookbackAhead lookback_read_ahead(const FusedArgs& p, uint32_t t) {
+  LookbackAhead a{0ull, 0ull, true};
+  const int64_t idx = int64_t(t) - 1 - threadIdx.x;
+  if (idx >= 0)
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
+                 : "=l"(a.agg), "=l"(a.incl)
+                 : "l"(&p.desc[idx].agg)
+                 : "memory");
+  return a;
+}
+
 template <class SmemT>
 __device__ unsigned long long lookback_block(SmemT& S, const FusedArgs& p, uint32_t t,
-                                             unsigned long long cnt, uint32_t& par) {
+                                             unsigned long long cnt, uint32_t& par,
+                                             LookbackAhead ahead = LookbackAhead{0ull, 0ull, false}) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   ChunkDesc* d = p.desc;
   unsigned long long pre = 0;
@@ -376,7 +395,12 @@ __device__ unsigned long long lookback_block(SmemT& S, const FusedArgs& p, uint3
     unsigned long long v = 0;
     if (idx >= 0) {
       unsigned long long va, vi;
-      asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(va), "=l"(vi) : "l"(&d[idx].agg) : "memory");
+      if (ahead.valid) {  // the first round, read ahead
+        va = ahead.agg;
+        vi = ahead.incl;
+      } else {
+        asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(va), "=l"(vi) : "l"(&d[idx].agg) : "memory");
+      }
       if (vi & kFlag) {
         v = vi & ~kFlag;
       } else if (va & kFlag) {
@@ -413,6 +437,7 @@ __device__ unsigned long long lookback_block(SmemT& S, const FusedArgs& p, uint3
       }
     }
     par ^= 1u;
+    ahead.valid = false;
     if (wait) {  // a chunk after the nearest prefix has published nothing yet
       if (++spins > (p.spin_limit ? p.spin_limit : kSpinLimit)) {
         if (tid == 0) raise_flag(p, &p.ctl->timeout, 1ull);

@@ -361,6 +361,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     unsigned long long nnz_acc = 0, cnt = 0, cnnz = 0;
     uint32_t fast_mask = 0, nslow = 0, ngen = 0;
     bool staged = false;
+    LookbackAhead ahead{0ull, 0ull, false};
     if (have) {
       // stage A's row pointers and ranges of the chunk (coalesced)
       uint64_t abase = 0;
@@ -520,6 +521,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       cnt = incl[crows - 1];
       if (tid == 0) atomicAdd(&p.ctl->nnz, cnnz);
       staged = stage != nullptr && cnt <= p.stage_cap;
+      // the pending chunk's look-back reads its first descriptors now, so
+      // the reads are in flight while the image is written
+      if (pend) ahead = lookback_read_ahead(p, S.pend_t[b ^ 1u]);
       if (staged) {
         // the chunk's image: fast rows from the slots, the rest recomputed
         uint32_t* img = stage + size_t(b) * (p.stage_cap + p.chunk_rows);
@@ -547,7 +551,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     if (pend) {
       const uint32_t pend_t = S.pend_t[b ^ 1u], pend_crows = S.pend_crows[b ^ 1u];
       const unsigned long long pend_cnt = S.pend_cnt[b ^ 1u];
-      const unsigned long long prefix = lookback_block(S, p, pend_t, pend_cnt, par);
+      const unsigned long long prefix = lookback_block(S, p, pend_t, pend_cnt, par, ahead);
       const uint32_t* img = stage + size_t(b ^ 1u) * (p.stage_cap + p.chunk_rows);
       const uint32_t* pincl = img + p.stage_cap;
       const uint32_t p0row = pend_t * p.chunk_rows;
