@@ -6,7 +6,9 @@
 // Boolean semiring (A+I)^(a+b) = (A+I)^a + A^a (A+I)^b, so with P_m = A^(2^m),
 // Q_0 = A + I and Q_(m+1) = Q_m + P_m Q_m the index
 // T = A^dlo (A+I)^(dup-dlo) is assembled from products whose left factor is a
-// power of A.  Every step is one launch of the row kernel computing
+// power of A.  For [400, 600]: P_1..P_8, Q_0..Q_7, two steps for the bits of
+// 200 above the lowest, two products for A^400 and the final one: 21 steps.
+// Every step is one launch of the row kernel computing
 // C = A B, C = D + A B or C = I + I A (= A + I), all canonical unions, so the
 // result equals the reference's index for canonical inputs (and for any input
 // when dlo > 0, where the last step is a product).
@@ -58,21 +60,12 @@ IndexPlan plan_index(unsigned dlo, unsigned dup) {
   for (int m = 1; m <= need_p; ++m) P.push_back(step(P[m - 1], false, P[m - 1], -1, false));
   int R = -1;  // (A+I)^e for the bits e of K handled so far (-1 with K = 0: the identity)
   if (K > 0) {
+    // the bits of K from the lowest: with e the bits taken so far,
+    // (A+I)^(2^m + e) = Q_m + P_m (A+I)^e, so every left factor is a power
+    // P_m, whose rows are a column or two
     int Q = step(-1, true, 0, -1, true);  // Q_0 = I + I A
-    int Ae = -1;                          // A^e when e has more than one bit
-    unsigned e = 0;
     for (int m = 0; m <= top_k; ++m) {
-      if ((K >> m) & 1u) {
-        if (R < 0) {
-          R = Q;
-          e = 1u << m;
-        } else {
-          const int Aexp = Ae >= 0 ? Ae : P[__builtin_ctz(e)];
-          R = step(Aexp, false, Q, R, false);  // (A+I)^(e + 2^m) = (A+I)^e + A^e Q_m
-          if ((K >> (m + 1)) != 0) Ae = step(Aexp, false, P[m], -1, false);
-          e += 1u << m;
-        }
-      }
+      if ((K >> m) & 1u) R = R < 0 ? Q : step(P[m], false, R, Q, false);
       if (m < top_k) Q = step(P[m], false, Q, Q, false);  // Q_(m+1) = Q_m + P_m Q_m
     }
   }
