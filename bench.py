@@ -44,11 +44,11 @@ sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
 L2_BYTES = 126 * 2**20
-# DRAM bytes (read + write) per C row of the row kernel, mean of the four
+# DRAM bytes (read + write) per C row of the row kernel, mean of the three
 # launches of the row kernel's ncu capture under profiles/ (10,019,292-row
 # graph): traffic scales with the rows of the product
-ROWMODE_TRAFFIC_BYTES_PER_ROW = (484213760 + 322915584 + 327040000 + 326183936 +
-                                 150529280 + 137050368 + 143670272 + 134789632) / 4 / 10019292
+ROWMODE_TRAFFIC_BYTES_PER_ROW = (487831040 + 323487744 + 326833408 +
+                                 154045184 + 137517312 + 142550272) / 3 / 10019292
 QUERY_ALG_BYTES = 33  # pair 8 B, two rowmap words 16 B, one range 8 B, answer 1 B
 
 
