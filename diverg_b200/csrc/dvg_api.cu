@@ -297,7 +297,8 @@ static dvg_matrix* range_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, boo
       for (dvg_matrix* m : lv) free_matrix(ctx, m);
     }
   } level_guard{ctx, levels};
-  if (!a_identity && !d && ctx->opt_levels && ctx->opt_spgemm_mode != 1 && a->nentries > 0 && b->nrows > 0) {
+  if (!a_identity && !d && ctx->opt_levels && ctx->opt_spgemm_mode != 1 && ctx->opt_spgemm_mode != 3 &&
+      a->nentries > 0 && b->nrows > 0) {
     const double mean = double(a->nnz) / double(a->nentries / 2);
     // automatic mode stages tiles above kWideRangeMean (faster there than
     // levels on the banded and power-of-(A+I) products measured); levels serve
@@ -767,7 +768,7 @@ dvg_status dvg_set_option(dvg_context* ctx, const char* key, int64_t value) {
       require(value == 0 || value == 1, "dindex_schedule must be 0 (sum of powers) or 1 (reference squaring)");
       ctx->opt_dindex_schedule = value;
     } else if (!std::strcmp(key, "spgemm_mode")) {
-      require(value >= 0 && value <= 2, "spgemm_mode must be 0 (automatic), 1 (tiled) or 2 (light)");
+      require(value >= 0 && value <= 3, "spgemm_mode must be 0 (automatic), 1 (tiled), 2 (light) or 3 (wide)");
       ctx->opt_spgemm_mode = value;
     } else if (!std::strcmp(key, "planned_build")) {
       require(value == 0 || value == 1, "planned_build must be 0 or 1");

@@ -173,6 +173,11 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
                          const std::vector<dvg_matrix*>* levels = nullptr);
 // C = U + S U with S the identity shifted by `shift` rows (row j of C is the
 // union of U's rows j and j + shift): one union level from the previous one.
+// The warp-per-row SpGEMM for rows that name many B ranges (dvg_spgemm_wide.cu):
+// desc holds spgemm_wide_desc_bytes(a->nrows) zeroed bytes, ticket a zeroed word.
+size_t spgemm_wide_desc_bytes(uint32_t nrows);
+void launch_spgemm_wide(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, const dvg_matrix* d,
+                        uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap, void* desc, unsigned* ticket);
 void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shift, uint64_t* c_rowmap,
                             uint32_t* c_entries, uint64_t cap);
 

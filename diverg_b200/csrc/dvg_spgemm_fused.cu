@@ -649,14 +649,19 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
                          const std::vector<dvg_matrix*>* levels) {
   const uint32_t n = a_identity ? b->nrows : a->nrows;
   if (n == 0) return;
-  // mode 1 forces the tile-staged kernel, mode 2 the row kernel; automatic
-  // (0) takes the tile-staged kernel when A's ranges are long on average (its
-  // block unions then replace most B-row visits) and the row kernel otherwise.
-  // An addend needs the row kernel.
+  // mode 1 forces the tile-staged kernel, mode 2 the row kernel, mode 3 the
+  // warp-per-row kernel; automatic (0) takes the warp-per-row kernel when A's
+  // ranges are long on average (a row then names many B ranges) and the row
+  // kernel otherwise.  An addend needs the row or the warp-per-row kernel.
+  const bool long_ranges = !a_identity && !(levels && !levels->empty()) && a->nentries > 0 &&
+                           double(a->nnz) > kWideRangeMean * double(a->nentries / 2);
+  if ((ctx->opt_spgemm_mode == 3 || (ctx->opt_spgemm_mode == 0 && long_ranges)) && !a_identity &&
+      !(levels && !levels->empty())) {
+    void* desc = chunk_scratch(ctx, spgemm_wide_desc_bytes(n));
+    launch_spgemm_wide(ctx, a, b, d, c_rowmap, c_entries, cap, desc, ctx->d_ticket);
+    return;
+  }
   bool row_mode = ctx->opt_spgemm_mode != 1;
-  if (ctx->opt_spgemm_mode == 0 && !a_identity && !d && !(levels && !levels->empty()) && a->nentries > 0 &&
-      double(a->nnz) > kWideRangeMean * double(a->nentries / 2))
-    row_mode = false;
   if (d && !row_mode) throw Error(DVG_ERR_INVALID_ARG, "fused spgemm: an addend needs the row kernel");
   if (row_mode) {
     // products that read union levels (long A ranges) have rows of many runs:

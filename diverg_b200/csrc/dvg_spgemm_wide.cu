@@ -1,0 +1,410 @@
+// dvg_spgemm_wide.cu -- range SpGEMM for products whose rows name many B
+// ranges (long A ranges over wide B rows): a warp per C row.
+//
+// Same result as the reference's symbolic + numeric SpGEMM
+// (include/diverg/range_sparse.hpp:1132-1442 in cartoonist/diverg, dispatched
+// by range_spgemm :2215-2281): row r of C is the union of the ranges of B
+// rows s..f for every range [s, f] of A's row r, emitted as sorted maximal
+// runs (merge rule start <= hi + 1).
+//
+// A warp takes a C row.  Its lanes load the row's A ranges and, for each, the
+// bounds of the B slice it names (B rows s..f are contiguous in B's entries),
+// all at once; the slices are then read with coalesced loads, a first time for
+// the row's column bounds and a second time (from L1) to OR every range into a
+// bitmap window of the warp in shared memory (two word masks a range, plus a
+// "reach" mark for the words a long range covers whole, as the reference's
+// HBitVector sets runs).  The runs come out of the window with the map01 /
+// map10 boundary masks of hbitvector.hpp:576-597 (gather_chunk); a row wider
+// than the window takes further windows.  The cost is per B range named, not
+// per column.
+//
+// Chunks of kWRows rows are taken from a ticket by persistent CTAs; the warps
+// of a CTA walk its rows (runs kept in a per-warp buffer), a chunk-local
+// prefix gives offsets, the chunk's aggregate is published and its image --
+// the whole chunk's output -- waits in shared memory to be resolved one
+// iteration later by a warp look-back (by then its predecessors have long
+// published), then written out with coalesced stores.  A chunk whose output
+// does not fit the image is resolved and written in its own iteration.  Reads
+// A and B once (plus L1 re-reads), writes C once.  Waits are bounded.
+#include "dvg_spgemm_common.cuh"
+
+namespace dvg {
+namespace {
+
+constexpr int kWThreads = 256;
+constexpr int kWWarps = kWThreads / 32;
+constexpr int kWRows = 64;     // rows of a chunk
+constexpr int kWWin = 128;     // window words of a warp (4,096 columns)
+constexpr int kWBuf = 256;     // run entries of a warp's rows kept from the count
+constexpr int kWImage = 2048;  // output entries of a chunk held for its deferred write-out
+
+struct WideSmem {
+  uint32_t bits[kWWarps][kWWin];
+  uint32_t reach[kWWarps][kWWin];
+  uint32_t buf[kWWarps][kWBuf];  // runs of the warp's rows of the counted chunk, in row order
+  uint32_t img[2][kWImage];      // images of the counted and the pending chunk
+  uint32_t incl[2][kWRows];      // their chunk-local inclusive row counts
+  uint32_t cnt_row[kWRows];      // entries of each row of the counted chunk
+  uint32_t kept[kWRows];         // 1: the row's runs are in its warp's buffer
+  unsigned long long prefix[2];  // exclusive prefixes: the pending chunk's, a chunk written in place
+  uint32_t pend_t[2], pend_rows[2], pend_cnt[2];
+  uint32_t next;
+  uint32_t cnt;
+};
+
+__device__ __forceinline__ void wide_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
+
+// Calls f(range) on this lane's share of the addend's ranges of `row` and of
+// every B range the row's A ranges name.  The slice bounds of the first 32 A
+// ranges are loaded once (by the lanes, together) and kept in b0 / b1.
+template <class F>
+__device__ __forceinline__ void wide_ranges(const FusedArgs& p, uint64_t row, uint64_t a0, uint64_t a1, uint64_t d0,
+                                            uint64_t d1, uint64_t b0, uint64_t b1, F&& f) {
+  const int lane = lane_id();
+  for (uint64_t t = d0 + lane; t < d1; t += 32) f(load_range(p.d_entries, t));
+  if (p.d_identity && lane == 0) f(make_uint2(uint32_t(row), uint32_t(row)));
+  for (uint64_t g = a0; g < a1; g += 32) {
+    uint64_t s0 = b0, s1 = b1;
+    if (g != a0) {  // a row of more than 32 A ranges: this group's slices
+      s0 = s1 = 0;
+      if (g + lane < a1) {
+        const uint2 ar = load_range(p.a_entries, g + lane);
+        if (ar.x <= ar.y) {
+          s0 = __ldg(p.b_rowmap + ar.x) >> 1;
+          s1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+        }
+      }
+    }
+    const uint32_t m = uint32_t(min(uint64_t(32), a1 - g));
+    for (uint32_t i = 0; i < m; ++i) {
+      const uint64_t t0 = __shfl_sync(kFullMask, s0, int(i)), t1 = __shfl_sync(kFullMask, s1, int(i));
+      uint64_t t = t0 + lane;
+      for (; t + 32 < t1; t += 64) {  // two loads in flight a lane
+        const uint2 x = load_range(p.b_entries, t), y = load_range(p.b_entries, t + 32);
+        f(x);
+        f(y);
+      }
+      if (t < t1) f(load_range(p.b_entries, t));
+    }
+  }
+}
+
+// One C row by the calling warp over its window (bits, reach): emits the
+// row's runs (entry k, value) and returns its entry count (the same on every
+// lane); adds the row's nnz to *nnz (each lane its words).
+template <class Emit>
+__device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, uint32_t* reach,
+                             unsigned long long* nnz, Emit&& emit) {
+  const int lane = lane_id();
+  const uint64_t a0 = __ldg(p.a_rowmap + row) >> 1, a1 = __ldg(p.a_rowmap + row + 1) >> 1;
+  uint64_t d0 = 0, d1 = 0;
+  if (p.d_rowmap) {
+    d0 = __ldg(p.d_rowmap + row) >> 1;
+    d1 = __ldg(p.d_rowmap + row + 1) >> 1;
+  }
+  uint64_t b0 = 0, b1 = 0;  // the slice of A range a0 + lane
+  if (a0 + lane < a1) {
+    const uint2 ar = load_range(p.a_entries, a0 + lane);
+    if (ar.x <= ar.y) {
+      b0 = __ldg(p.b_rowmap + ar.x) >> 1;
+      b1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
+    }
+  }
+  uint32_t mn = 0xffffffffu, mx = 0;
+  wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
+    if (r.y < r.x) return;
+    mn = min(mn, r.x);
+    mx = max(mx, r.y);
+  });
+  mn = group_min<32>(kFullMask, mn);
+  mx = group_max<32>(kFullMask, mx);
+  if (mn > mx) return 0;
+  uint64_t count = 0;
+  const uint64_t base = mn & ~31u;
+  const uint64_t nw_total = ((uint64_t(mx) - base) >> 5) + 2;
+  uint32_t carry = 0;
+  for (uint64_t w0 = 0; w0 < nw_total; w0 += kWWin) {
+    const uint32_t nwc = uint32_t(min(uint64_t(kWWin), nw_total - w0));
+    const uint64_t cb = base + 32 * w0;
+    const uint64_t ce = cb + 32ull * nwc - 1;
+    for (uint32_t w = lane; w < nwc; w += 32) {
+      bits[w] = 0;
+      reach[w] = 0;
+    }
+    __syncwarp();
+    wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
+      const uint64_t cs = max(uint64_t(r.x), cb);
+      const uint64_t cf = min(uint64_t(r.y), ce);
+      if (cs > cf || r.y < r.x) return;
+      const uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
+      const uint32_t lo = ~0u << (cs & 31);
+      const uint32_t hi = ~0u >> (31 - (cf & 31));
+      if (ws == we) {
+        atomicOr(bits + ws, lo & hi);
+      } else {
+        atomicOr(bits + ws, lo);
+        atomicOr(bits + we, hi);
+        if (we > ws + 1) atomicMax(reach + ws + 1, we);
+      }
+    });
+    __syncwarp();
+    uint32_t run_reach = 0;
+    for (uint32_t wb = 0; wb < nwc; wb += 32) {
+      const uint32_t w = wb + lane;
+      const bool valid = w < nwc;
+      uint32_t x = 0, rr = 0;
+      if (valid) {
+        x = bits[w];
+        rr = reach[w];
+      }
+      rr = group_incl_max<32>(kFullMask, rr, lane);
+      rr = max(rr, run_reach);
+      if (valid && rr > w) x = ~0u;
+      run_reach = __shfl_sync(kFullMask, rr, 31);
+      if (nnz) *nnz += __popc(x);
+      const uint32_t last = min(31u, nwc - 1 - wb);
+      count += gather_chunk(x, valid, cb + 32ull * w, 32, lane, kFullMask, carry, count, last, emit);
+    }
+    __syncwarp();
+  }
+  return count;
+}
+
+// Warp 0 walks back from chunk t (its aggregate published) to the nearest
+// inclusive prefix, publishes t's inclusive prefix (and, for the last chunk,
+// the product's total, with the overflow check) and leaves t's exclusive
+// prefix in *out; the caller's barrier makes it visible.  Bounded.
+__device__ void wide_lookback(unsigned long long* out, const FusedArgs& p, uint32_t t, unsigned long long cnt) {
+  const int lane = lane_id();
+  ChunkDesc* d = p.desc;
+  unsigned long long pre = 0;
+  int64_t j = int64_t(t) - 1;
+  uint32_t spins = 0;
+  const uint32_t limit = p.spin_limit ? p.spin_limit : kSpinLimit;
+  while (j >= 0) {
+    const int64_t idx = j - lane;
+    int st = 2;  // 2: inclusive prefix (or before chunk 0), 1: aggregate, 0: nothing yet
+    unsigned long long v = 0;
+    if (idx >= 0) {
+      unsigned long long va, vi;
+      asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(va), "=l"(vi) : "l"(&d[idx].agg) : "memory");
+      if (vi & kFlag) {
+        v = vi & ~kFlag;
+      } else if (va & kFlag) {
+        st = 1;
+        v = va & ~kFlag;
+      } else {
+        st = 0;
+      }
+    }
+    const unsigned im = __ballot_sync(kFullMask, st == 2), wm = __ballot_sync(kFullMask, st == 0);
+    const int fi = im ? __ffs(im) - 1 : 32;
+    const unsigned before = fi == 32 ? kFullMask : ((1u << fi) - 1u);
+    if (wm & before) {
+      if (++spins > limit) {
+        if (lane == 0) raise_flag(p, &p.ctl->timeout, 1ull);
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    unsigned long long sv = lane <= fi ? v : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(kFullMask, sv, o);
+    pre += sv;
+    if (fi < 32) break;
+    j -= 32;
+  }
+  if (lane == 0) {
+    st_relaxed(&d[t].incl, kFlag | (pre + cnt));
+    *out = pre;
+    if (t == p.nchunks - 1) {
+      p.ctl->total = pre + cnt;
+      if (pre + cnt > p.cap) raise_flag(p, &p.ctl->overflow, pre + cnt);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kWThreads) k_spgemm_wide(FusedArgs p) {
+  extern __shared__ __align__(16) unsigned char wide_smem_raw[];
+  WideSmem& S = *reinterpret_cast<WideSmem*>(wide_smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* const bits = S.bits[warp];
+  uint32_t* const reach = S.reach[warp];
+  uint32_t* const buf = S.buf[warp];
+  unsigned long long nnz_acc = 0;
+  if (tid == 0) S.next = atomicAdd(p.ticket, 1u);
+  wide_sync();
+  uint32_t t = S.next, b = 0;
+  bool pend = false;  // a counted chunk waits in image buffer b ^ 1
+  while (t < p.nchunks || pend) {
+    const bool have = t < p.nchunks;
+    const uint32_t c0 = have ? t * uint32_t(kWRows) : 0u;
+    const uint32_t crows = have ? min(uint32_t(kWRows), p.nrows - c0) : 0u;
+    uint32_t cnt = 0;
+    bool imaged = false;
+    if (have) {
+      // 1. count: warp w walks rows w, w + kWWarps, ...; their runs go to its buffer
+      uint32_t bpos = 0;
+      for (uint32_t r = warp; r < crows; r += kWWarps) {
+        const uint32_t start = bpos;
+        const uint64_t c = wide_row(p, uint64_t(c0) + r, bits, reach, &nnz_acc, [&](uint64_t k, uint32_t v) {
+          if (start + k < uint64_t(kWBuf)) buf[start + k] = v;
+        });
+        const bool kept = start + c <= uint64_t(kWBuf);
+        if (c > 0xffffffffull) raise_flag(p, &p.ctl->status, 16ull);
+        if (lane == 0) {
+          S.cnt_row[r] = uint32_t(c);
+          S.kept[r] = kept ? 1u : 0u;
+        }
+        if (kept) bpos += uint32_t(c);
+      }
+      wide_sync();
+      // 2. chunk-local prefix (warp 0: two rows a lane)
+      if (warp == 0) {
+        const uint32_t r0 = 2 * lane, r1 = 2 * lane + 1;
+        const uint32_t v0 = r0 < crows ? S.cnt_row[r0] : 0u, v1 = r1 < crows ? S.cnt_row[r1] : 0u;
+        uint64_t incl = uint64_t(v0) + v1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint64_t u = __shfl_up_sync(kFullMask, incl, o);
+          if (lane >= o) incl += u;
+        }
+        const uint64_t total = __shfl_sync(kFullMask, incl, 31);
+        if (total > 0xffffffffull) {
+          if (lane == 0) raise_flag(p, &p.ctl->status, 16ull);
+        }
+        if (r0 < crows) S.incl[b][r0] = uint32_t(incl - v1);
+        if (r1 < crows) S.incl[b][r1] = uint32_t(incl);
+        if (lane == 0) {
+          S.cnt = uint32_t(total);
+          publish_aggregate(p, t, total);
+          S.next = atomicAdd(p.ticket, 1u);  // the next chunk, taken once this one is counted
+        }
+      }
+      wide_sync();
+      cnt = S.cnt;
+      // 3. the chunk's image in buffer b: kept rows copied, the rest walked again
+      imaged = cnt <= uint32_t(kWImage);
+      if (imaged) {
+        uint32_t* img = S.img[b];
+        uint32_t bp = 0;
+        for (uint32_t r = warp; r < crows; r += kWWarps) {
+          const uint32_t n = S.cnt_row[r], o = r ? S.incl[b][r - 1] : 0u;
+          if (S.kept[r]) {
+            for (uint32_t k = lane; k < n; k += 32) img[o + k] = buf[bp + k];
+            bp += n;
+          } else {
+            bool bad = false;
+            const uint64_t c = wide_row(p, uint64_t(c0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
+              if (k < n) img[o + k] = v;
+              else bad = true;
+            });
+            if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+          }
+        }
+      }
+    }
+    // 4. the pending chunk (counted last iteration): look-back, row map, entries
+    if (pend) {
+      const uint32_t pt = S.pend_t[b ^ 1u], prow = S.pend_rows[b ^ 1u], pcnt = S.pend_cnt[b ^ 1u];
+      if (warp == 0) wide_lookback(&S.prefix[0], p, pt, pcnt);
+      wide_sync();
+      const unsigned long long prefix = S.prefix[0];
+      for (uint32_t r = tid; r < prow; r += kWThreads)
+        p.c_rowmap[uint64_t(pt) * kWRows + r + 1] = prefix + S.incl[b ^ 1u][r];
+      if (pt == 0 && tid == 0) p.c_rowmap[0] = 0;
+      if (prefix + pcnt <= p.cap) {
+        uint32_t* dst = p.c_entries + prefix;
+        for (uint32_t k = tid; k < pcnt; k += kWThreads) dst[k] = S.img[b ^ 1u][k];
+      } else if (tid == 0 && pcnt) {
+        raise_flag(p, &p.ctl->overflow, 1ull);
+      }
+      pend = false;
+    }
+    // 5. a chunk whose output does not fit its image: resolved now, in place
+    if (have && !imaged) {
+      if (warp == 0) wide_lookback(&S.prefix[1], p, t, cnt);
+      wide_sync();
+      const unsigned long long prefix = S.prefix[1];
+      for (uint32_t r = tid; r < crows; r += kWThreads) p.c_rowmap[uint64_t(c0) + r + 1] = prefix + S.incl[b][r];
+      if (t == 0 && tid == 0) p.c_rowmap[0] = 0;
+      uint32_t bp = 0;
+      for (uint32_t r = warp; r < crows; r += kWWarps) {
+        const uint32_t n = S.cnt_row[r], o = r ? S.incl[b][r - 1] : 0u;
+        const bool kept = S.kept[r] != 0;
+        if (n && prefix + o + n > p.cap) {
+          if (lane == 0) raise_flag(p, &p.ctl->overflow, 1ull);
+        } else if (kept) {
+          uint32_t* dst = p.c_entries + prefix + o;
+          for (uint32_t k = lane; k < n; k += 32) dst[k] = buf[bp + k];
+        } else if (n) {
+          uint32_t* dst = p.c_entries + prefix + o;
+          bool bad = false;
+          const uint64_t c = wide_row(p, uint64_t(c0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
+            if (k < n) dst[k] = v;
+            else bad = true;
+          });
+          if (bad || c != n) raise_flag(p, &p.ctl->status, 8ull);
+        }
+        if (kept) bp += n;
+      }
+    }
+    if (have && imaged) {
+      if (tid == 0) {
+        S.pend_t[b] = t;
+        S.pend_rows[b] = crows;
+        S.pend_cnt[b] = cnt;
+      }
+      pend = true;
+      b ^= 1u;
+    }
+    // every thread is done with the buffers and images it needs; S.next and
+    // the pending record are visible
+    wide_sync();
+    t = have ? S.next : 0xffffffffu;
+  }
+  // the product's nnz: one atomic per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nnz_acc += __shfl_xor_sync(kFullMask, nnz_acc, o);
+  if (lane == 0 && nnz_acc) atomicAdd(&p.ctl->nnz, nnz_acc);
+}
+
+}  // namespace
+
+size_t spgemm_wide_desc_bytes(uint32_t nrows) {
+  return size_t((uint64_t(nrows) + kWRows - 1) / kWRows) * sizeof(ChunkDesc);
+}
+
+void launch_spgemm_wide(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, const dvg_matrix* d,
+                        uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap, void* desc, unsigned* ticket) {
+  const uint32_t n = a->nrows;
+  if (n == 0) return;
+  FusedArgs p{};
+  p.a_rowmap = a->rowmap;
+  p.a_entries = a->entries;
+  p.b_rowmap = b->rowmap;
+  p.b_entries = b->entries;
+  p.d_rowmap = d ? d->rowmap : nullptr;
+  p.d_entries = d ? d->entries : nullptr;
+  p.c_rowmap = c_rowmap;
+  p.c_entries = c_entries;
+  p.cap = cap;
+  p.desc = static_cast<ChunkDesc*>(desc);
+  p.ticket = ticket;
+  p.ctl = ctx->d_ctl;
+  p.nrows = n;
+  p.chunk_rows = kWRows;
+  p.nchunks = uint32_t((uint64_t(n) + kWRows - 1) / kWRows);
+  const int smem = int(sizeof(WideSmem));
+  DVG_CUDA(cudaFuncSetAttribute(k_spgemm_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  DVG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spgemm_wide, kWThreads, smem));
+  if (per_sm < 1) throw Error(DVG_ERR_DEVICE, "wide spgemm: shared memory layout does not fit");
+  const unsigned grid = unsigned(std::min<uint64_t>(p.nchunks, uint64_t(per_sm) * ctx->num_sms));
+  k_spgemm_wide<<<grid, kWThreads, smem, ctx->stream>>>(p);
+  DVG_CUDA(cudaGetLastError());
+  ctx->stats.kernel_launches++;
+}
+
+}  // namespace dvg
