@@ -110,6 +110,66 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
       b1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
     }
   }
+  // First one window, anchored half a window before the row's first B range
+  // (or addend range): when every range falls inside it (all but the last
+  // word, which closes the last run), one pass over the ranges makes the row.
+  {
+    const unsigned nonempty = __ballot_sync(kFullMask, b1 > b0);
+    uint32_t s0 = 0xffffffffu;
+    if (nonempty) {
+      const int l = __ffs(nonempty) - 1;
+      const uint64_t t = __shfl_sync(kFullMask, b0, l);
+      if (lane == 0) s0 = load_range(p.b_entries, t).x;
+    } else if (d1 > d0) {
+      if (lane == 0) s0 = load_range(p.d_entries, d0).x;
+    }
+    s0 = __shfl_sync(kFullMask, s0, 0);
+    if (s0 != 0xffffffffu) {
+      const uint64_t cb = (s0 >= 32u * (kWWin / 2) ? uint64_t(s0) - 32u * (kWWin / 2) : 0ull) & ~31ull;
+      const uint64_t ce = cb + 32ull * (kWWin - 1) - 1;  // the last word stays empty
+      for (uint32_t w = lane; w < uint32_t(kWWin); w += 32) {
+        bits[w] = 0;
+        reach[w] = 0;
+      }
+      __syncwarp();
+      bool out = false;
+      wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
+        if (r.y < r.x) return;
+        if (r.x < cb || r.y > ce) {
+          out = true;
+          return;
+        }
+        const uint32_t ws = uint32_t((r.x - cb) >> 5), we = uint32_t((r.y - cb) >> 5);
+        const uint32_t lo = ~0u << (r.x & 31);
+        const uint32_t hi = ~0u >> (31 - (r.y & 31));
+        if (ws == we) {
+          atomicOr(bits + ws, lo & hi);
+        } else {
+          atomicOr(bits + ws, lo);
+          atomicOr(bits + we, hi);
+          if (we > ws + 1) atomicMax(reach + ws + 1, we);
+        }
+      });
+      __syncwarp();
+      if (!__any_sync(kFullMask, out)) {
+        uint64_t count = 0;
+        uint32_t carry = 0, run_reach = 0;
+        for (uint32_t wb = 0; wb < uint32_t(kWWin); wb += 32) {
+          const uint32_t w = wb + lane;
+          uint32_t x = bits[w], rr = reach[w];
+          rr = group_incl_max<32>(kFullMask, rr, lane);
+          rr = max(rr, run_reach);
+          if (rr > w) x = ~0u;
+          run_reach = __shfl_sync(kFullMask, rr, 31);
+          if (nnz) *nnz += __popc(x);
+          count += gather_chunk(x, true, cb + 32ull * w, 32, lane, kFullMask, carry, count, 31u, emit);
+        }
+        __syncwarp();
+        return count;
+      }
+    }
+  }
+  // the general form: the row's column bounds first, then windows over them
   uint32_t mn = 0xffffffffu, mx = 0;
   wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
     if (r.y < r.x) return;
@@ -225,7 +285,7 @@ __device__ void wide_lookback(unsigned long long* out, const FusedArgs& p, uint3
   }
 }
 
-__global__ void __launch_bounds__(kWThreads) k_spgemm_wide(FusedArgs p) {
+__global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char wide_smem_raw[];
   WideSmem& S = *reinterpret_cast<WideSmem*>(wide_smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
