@@ -124,24 +124,30 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
       if (lane == 0) s0 = load_range(p.d_entries, d0).x;
     }
     s0 = __shfl_sync(kFullMask, s0, 0);
-    if (s0 != 0xffffffffu) {
-      const uint64_t cb = (s0 >= 32u * (kWWin / 2) ? uint64_t(s0) - 32u * (kWWin / 2) : 0ull) & ~31ull;
-      const uint64_t ce = cb + 32ull * (kWWin - 1) - 1;  // the last word stays empty
+    // (window words and the columns they start at in 32 bits: columns are
+    // below 2^32 - 2, and a window starting past them would hold nothing)
+    if (s0 != 0xffffffffu && s0 < 0xffffffffu - 32u * kWWin) {
+      const uint32_t cb = (s0 >= 32u * (kWWin / 2) ? s0 - 32u * (kWWin / 2) : 0u) & ~31u;
+      const uint32_t span = 32u * (kWWin - 1);  // the last word stays empty
       for (uint32_t w = lane; w < uint32_t(kWWin); w += 32) {
         bits[w] = 0;
         reach[w] = 0;
       }
       __syncwarp();
       bool out = false;
+      uint32_t top = 0, bottom = kWWin;  // words in [bottom, top) hold bits
       wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
         if (r.y < r.x) return;
-        if (r.x < cb || r.y > ce) {
+        const uint32_t xs = r.x - cb, xe = r.y - cb;  // wrap when r.x < cb: then out of the window
+        if (xs >= span || xe >= span) {
           out = true;
           return;
         }
-        const uint32_t ws = uint32_t((r.x - cb) >> 5), we = uint32_t((r.y - cb) >> 5);
-        const uint32_t lo = ~0u << (r.x & 31);
-        const uint32_t hi = ~0u >> (31 - (r.y & 31));
+        const uint32_t ws = xs >> 5, we = xe >> 5;
+        const uint32_t lo = ~0u << (xs & 31);
+        const uint32_t hi = ~0u >> (31 - (xe & 31));
+        top = max(top, we + 1);
+        bottom = min(bottom, ws);
         if (ws == we) {
           atomicOr(bits + ws, lo & hi);
         } else {
@@ -152,17 +158,26 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
       });
       __syncwarp();
       if (!__any_sync(kFullMask, out)) {
+        // words from the first to one past the last touched: runs close there
+        const uint32_t nw = min(uint32_t(kWWin), group_max<32>(kFullMask, top) + 1);
+        const uint32_t w_first = group_min<32>(kFullMask, bottom) & ~31u;  // below: empty words
         uint64_t count = 0;
         uint32_t carry = 0, run_reach = 0;
-        for (uint32_t wb = 0; wb < uint32_t(kWWin); wb += 32) {
+        for (uint32_t wb = w_first; wb < nw; wb += 32) {
           const uint32_t w = wb + lane;
-          uint32_t x = bits[w], rr = reach[w];
+          const bool valid = w < nw;
+          uint32_t x = 0, rr = 0;
+          if (valid) {
+            x = bits[w];
+            rr = reach[w];
+          }
           rr = group_incl_max<32>(kFullMask, rr, lane);
           rr = max(rr, run_reach);
-          if (rr > w) x = ~0u;
+          if (valid && rr > w) x = ~0u;
           run_reach = __shfl_sync(kFullMask, rr, 31);
           if (nnz) *nnz += __popc(x);
-          count += gather_chunk(x, true, cb + 32ull * w, 32, lane, kFullMask, carry, count, 31u, emit);
+          count += gather_chunk(x, valid, uint64_t(cb) + 32ull * w, 32, lane, kFullMask, carry, count,
+                                min(31u, nw - 1 - wb), emit);
         }
         __syncwarp();
         return count;
