@@ -1059,6 +1059,14 @@ dvg_status dvg_selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit) {
   });
 }
 
+dvg_status dvg_calibrate_range_ops(dvg_context* ctx, double* ops_per_second) {
+  return guarded([&] {
+    require(ctx != nullptr && ops_per_second != nullptr, "null argument");
+    Lock lk(ctx);
+    *ops_per_second = calibrate_range_ops(ctx);
+  });
+}
+
 dvg_status dvg_adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uint32_t* node_len, uint64_t nedges,
                                     const uint32_t* edges, uint32_t lower, uint32_t upper, dvg_matrix** out) {
   return guarded([&] {

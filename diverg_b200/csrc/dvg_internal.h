@@ -178,6 +178,9 @@ void launch_spgemm_fused(dvg_context* ctx, const dvg_matrix* a, bool a_identity,
 size_t spgemm_wide_desc_bytes(uint32_t nrows);
 void launch_spgemm_wide(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix* b, const dvg_matrix* d,
                         uint64_t* c_rowmap, uint32_t* c_entries, uint64_t cap, void* desc, unsigned* ticket);
+// Range operations a second the warp-per-row kernel's inner work sustains on
+// this device (measured; synchronises the context's stream).
+double calibrate_range_ops(dvg_context* ctx);
 void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shift, uint64_t* c_rowmap,
                             uint32_t* c_entries, uint64_t cap);
 

@@ -483,3 +483,131 @@ void launch_spgemm_wide(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix*
 }
 
 }  // namespace dvg
+
+// ---- the on-chip rate of a range operation ------------------------------------
+//
+// The measured denominator of this kernel's on-chip roofline: warps OR 8-byte
+// ranges, read from a small table that stays in L1/L2, into their bitmap
+// windows exactly as wide_row does (masks, reach marks, shared atomics), 512
+// ranges a "row", and take each row's runs out of the window with the same
+// gather -- the work of a range operation with none of the A / B indirection,
+// the chunk bookkeeping or the write-out.  Ranges lie within 2,048 columns and
+// are up to 63 columns long, as in the banded microbenchmark.
+namespace dvg {
+namespace {
+
+constexpr uint32_t kCalRanges = 4096;
+constexpr uint32_t kCalRowsPerWarp = 256;
+
+__global__ void k_rangeop_table(uint2* t) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kCalRanges) return;
+  uint32_t h = i * 2654435761u + 12345u;
+  h ^= h >> 15;
+  h *= 2246822519u;
+  h ^= h >> 13;
+  const uint32_t s = h % 1984u;
+  t[i] = make_uint2(s, s + ((h >> 16) & 63u));
+}
+
+__global__ void __launch_bounds__(kWThreads, 4) k_rangeop_calibrate(const uint2* __restrict__ table,
+                                                                    unsigned long long* sink) {
+  __shared__ uint32_t cal_bits[kWWarps][kWWin];
+  __shared__ uint32_t cal_reach[kWWarps][kWWin];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* bits = cal_bits[warp];
+  uint32_t* reach = cal_reach[warp];
+  const uint32_t gw = blockIdx.x * kWWarps + warp;
+  unsigned long long total = 0, nnz = 0;
+  for (uint32_t row = 0; row < kCalRowsPerWarp; ++row) {
+    for (uint32_t w = lane; w < uint32_t(kWWin); w += 32) {
+      bits[w] = 0;
+      reach[w] = 0;
+    }
+    __syncwarp();
+    uint32_t top = 0;
+    const uint32_t base = gw * 131u + row * 517u;
+    for (uint32_t it = 0; it < 16; it += 2) {
+      const uint2 x = __ldg(table + ((base + it * 32 + lane) & (kCalRanges - 1)));
+      const uint2 y = __ldg(table + ((base + (it + 1) * 32 + lane) & (kCalRanges - 1)));
+      for (const uint2 r : {x, y}) {
+        const uint32_t ws = r.x >> 5, we = r.y >> 5;
+        const uint32_t lo = ~0u << (r.x & 31);
+        const uint32_t hi = ~0u >> (31 - (r.y & 31));
+        top = max(top, we + 1);
+        if (ws == we) {
+          atomicOr(bits + ws, lo & hi);
+        } else {
+          atomicOr(bits + ws, lo);
+          atomicOr(bits + we, hi);
+          if (we > ws + 1) atomicMax(reach + ws + 1, we);
+        }
+      }
+    }
+    __syncwarp();
+    const uint32_t nw = min(uint32_t(kWWin), group_max<32>(kFullMask, top) + 1);
+    uint64_t count = 0;
+    uint32_t carry = 0, run_reach = 0;
+    for (uint32_t wb = 0; wb < nw; wb += 32) {
+      const uint32_t w = wb + lane;
+      const bool valid = w < nw;
+      uint32_t x = 0, rr = 0;
+      if (valid) {
+        x = bits[w];
+        rr = reach[w];
+      }
+      rr = group_incl_max<32>(kFullMask, rr, lane);
+      rr = max(rr, run_reach);
+      if (valid && rr > w) x = ~0u;
+      run_reach = __shfl_sync(kFullMask, rr, 31);
+      nnz += __popc(x);
+      count += gather_chunk(x, valid, 32ull * w, 32, lane, kFullMask, carry, count, min(31u, nw - 1 - wb),
+                            [](uint64_t, uint32_t) {});
+    }
+    __syncwarp();
+    total += count;
+  }
+  // keeps the work observable
+  if (lane == 0) atomicAdd(sink, total + (nnz & 1ull));
+}
+
+}  // namespace
+
+double calibrate_range_ops(dvg_context* ctx) {
+  void* mem = dalloc(ctx, kCalRanges * sizeof(uint2) + 256);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float best = 0.f;
+  try {
+    auto* table = static_cast<uint2*>(mem);
+    auto* sink = reinterpret_cast<unsigned long long*>(static_cast<char*>(mem) + kCalRanges * sizeof(uint2));
+    DVG_CUDA(cudaMemsetAsync(sink, 0, 8, ctx->stream));
+    k_rangeop_table<<<(kCalRanges + 255) / 256, 256, 0, ctx->stream>>>(table);
+    DVG_CUDA(cudaGetLastError());
+    DVG_CUDA(cudaEventCreate(&e0));
+    DVG_CUDA(cudaEventCreate(&e1));
+    const unsigned grid = unsigned(4 * ctx->num_sms);
+    for (int rep = 0; rep < 4; ++rep) {  // the first is a warm-up; the best of the rest
+      DVG_CUDA(cudaEventRecord(e0, ctx->stream));
+      k_rangeop_calibrate<<<grid, kWThreads, 0, ctx->stream>>>(table, sink);
+      DVG_CUDA(cudaGetLastError());
+      DVG_CUDA(cudaEventRecord(e1, ctx->stream));
+      DVG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      DVG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0 && (best == 0.f || ms < best)) best = ms;
+    }
+    ctx->stats.kernel_launches += 5;
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    dfree(ctx, mem);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(ctx, mem);
+  const double ops = double(4 * ctx->num_sms) * kWWarps * kCalRowsPerWarp * 512.0;
+  return best > 0.f ? ops / (double(best) * 1e-3) : 0.0;
+}
+
+}  // namespace dvg

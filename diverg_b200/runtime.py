@@ -59,6 +59,13 @@ class Context:
     def reset_stats(self):
         N.check(N.lib().dvg_stats_reset(self.handle))
 
+    def calibrate_range_ops(self):
+        """Range operations a second the device sustains for the warp-per-row
+        SpGEMM's inner work (the denominator of its on-chip roofline)."""
+        v = ctypes.c_double()
+        N.check(N.lib().dvg_calibrate_range_ops(self.handle, ctypes.byref(v)))
+        return v.value
+
     # -- matrices ---------------------------------------------------------------
     def upload(self, m: CRSMatrix) -> "DeviceMatrix":
         L = N.lib()

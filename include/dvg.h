@@ -189,6 +189,17 @@ dvg_status dvg_batch_distance_index(dvg_context* ctx, uint32_t ngraphs, const dv
  * DVG_ERR_TIMEOUT; any other status means the bound did not hold. */
 dvg_status dvg_selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit);
 
+/* ---- the on-chip rate of a range operation
+ *
+ * No counterpart in the reference: a measurement for the roofline of the
+ * warp-per-row SpGEMM (products with long A ranges), whose bound is on-chip
+ * work, not HBM.  Times warps that OR ranges held in L1/L2 into bitmap
+ * windows in shared memory and take the runs out, exactly the kernel's inner
+ * work without its A / B indirection or write-out, and stores the range
+ * operations a second the device sustained.  Synchronises the context's
+ * stream. */
+dvg_status dvg_calibrate_range_ops(dvg_context* ctx, double* ops_per_second);
+
 /* ---- adjacency construction: util::range_adjacency_matrix
  *      (adjacency.hpp:249-265) over util::adjacency_matrix (:170-228) and the
  *      Basic->Range conversion of crs_matrix::append (crs_matrix.hpp:197-242)

@@ -11,8 +11,9 @@ from tests.conftest import load_golden
 pytestmark = pytest.mark.gpu
 
 # (algo, group lanes, window words, SpGEMM mode): the single-pass kernels in
-# their automatic choice, the tile-staged rows and the thread-per-row mode
-FUSED = [(0, 0, 0, 0), (0, 0, 0, 1), (0, 0, 0, 2)]
+# their automatic choice, the tile-staged rows, the thread-per-row mode and
+# the warp-per-row mode
+FUSED = [(0, 0, 0, 0), (0, 0, 0, 1), (0, 0, 0, 2), (0, 0, 0, 3)]
 PLANS = FUSED
 
 

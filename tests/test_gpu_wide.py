@@ -126,3 +126,12 @@ def test_automatic_choice_takes_the_warp_per_row_kernel(ctx):
     ctx.spgemm(ctx.upload(a), ctx.upload(a)).free()
     st = ctx.stats()
     assert st["spgemm_calls"] == 1 and st["spgemm_light"] == 0 and st["spgemm_levels"] == 0, st
+
+
+def test_range_operation_calibration(ctx):
+    # the on-chip denominator: positive and finite, and the context computes
+    # correctly afterwards
+    rate = ctx.calibrate_range_ops()
+    assert np.isfinite(rate) and 1e9 < rate < 1e14, rate
+    a = gen.banded(1 << 12, 64, 4.0, 16.0, seed=13)
+    assert_same(product(ctx, a, a), orc.spgemm(omat(a), omat(a)), "after calibration")
