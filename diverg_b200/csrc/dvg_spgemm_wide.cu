@@ -54,197 +54,6 @@ struct WideSmem {
 
 __device__ __forceinline__ void wide_sync() { asm volatile("barrier.sync 0;" ::: "memory"); }
 
-// Calls f(range) on this lane's share of the addend's ranges of `row` and of
-// every B range the row's A ranges name.  The slice bounds of the first 32 A
-// ranges are loaded once (by the lanes, together) and kept in b0 / b1.
-template <class F>
-__device__ __forceinline__ void wide_ranges(const FusedArgs& p, uint64_t row, uint64_t a0, uint64_t a1, uint64_t d0,
-                                            uint64_t d1, uint64_t b0, uint64_t b1, F&& f) {
-  const int lane = lane_id();
-  for (uint64_t t = d0 + lane; t < d1; t += 32) f(load_range(p.d_entries, t));
-  if (p.d_identity && lane == 0) f(make_uint2(uint32_t(row), uint32_t(row)));
-  for (uint64_t g = a0; g < a1; g += 32) {
-    uint64_t s0 = b0, s1 = b1;
-    if (g != a0) {  // a row of more than 32 A ranges: this group's slices
-      s0 = s1 = 0;
-      if (g + lane < a1) {
-        const uint2 ar = load_range(p.a_entries, g + lane);
-        if (ar.x <= ar.y) {
-          s0 = __ldg(p.b_rowmap + ar.x) >> 1;
-          s1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-        }
-      }
-    }
-    const uint32_t m = uint32_t(min(uint64_t(32), a1 - g));
-    for (uint32_t i = 0; i < m; ++i) {
-      const uint64_t t0 = __shfl_sync(kFullMask, s0, int(i)), t1 = __shfl_sync(kFullMask, s1, int(i));
-      uint64_t t = t0 + lane;
-      for (; t + 32 < t1; t += 64) {  // two loads in flight a lane
-        const uint2 x = load_range(p.b_entries, t), y = load_range(p.b_entries, t + 32);
-        f(x);
-        f(y);
-      }
-      if (t < t1) f(load_range(p.b_entries, t));
-    }
-  }
-}
-
-// One C row by the calling warp over its window (bits, reach): emits the
-// row's runs (entry k, value) and returns its entry count (the same on every
-// lane); adds the row's nnz to *nnz (each lane its words).
-template <class Emit>
-__device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, uint32_t* reach,
-                             unsigned long long* nnz, Emit&& emit) {
-  const int lane = lane_id();
-  const uint64_t a0 = __ldg(p.a_rowmap + row) >> 1, a1 = __ldg(p.a_rowmap + row + 1) >> 1;
-  uint64_t d0 = 0, d1 = 0;
-  if (p.d_rowmap) {
-    d0 = __ldg(p.d_rowmap + row) >> 1;
-    d1 = __ldg(p.d_rowmap + row + 1) >> 1;
-  }
-  uint64_t b0 = 0, b1 = 0;  // the slice of A range a0 + lane
-  if (a0 + lane < a1) {
-    const uint2 ar = load_range(p.a_entries, a0 + lane);
-    if (ar.x <= ar.y) {
-      b0 = __ldg(p.b_rowmap + ar.x) >> 1;
-      b1 = __ldg(p.b_rowmap + uint64_t(ar.y) + 1) >> 1;
-    }
-  }
-  // First one window, anchored half a window before the row's first B range
-  // (or addend range): when every range falls inside it (all but the last
-  // word, which closes the last run), one pass over the ranges makes the row.
-  {
-    const unsigned nonempty = __ballot_sync(kFullMask, b1 > b0);
-    uint32_t s0 = 0xffffffffu;
-    if (nonempty) {
-      const int l = __ffs(nonempty) - 1;
-      const uint64_t t = __shfl_sync(kFullMask, b0, l);
-      if (lane == 0) s0 = load_range(p.b_entries, t).x;
-    } else if (d1 > d0) {
-      if (lane == 0) s0 = load_range(p.d_entries, d0).x;
-    }
-    s0 = __shfl_sync(kFullMask, s0, 0);
-    // (window words and the columns they start at in 32 bits: columns are
-    // below 2^32 - 2, and a window starting past them would hold nothing)
-    if (s0 != 0xffffffffu && s0 < 0xffffffffu - 32u * kWWin) {
-      const uint32_t cb = (s0 >= 32u * (kWWin / 2) ? s0 - 32u * (kWWin / 2) : 0u) & ~31u;
-      const uint32_t span = 32u * (kWWin - 1);  // the last word stays empty
-      for (uint32_t w = lane; w < uint32_t(kWWin); w += 32) {
-        bits[w] = 0;
-        reach[w] = 0;
-      }
-      __syncwarp();
-      bool out = false;
-      uint32_t top = 0, bottom = kWWin;  // words in [bottom, top) hold bits
-      wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
-        if (r.y < r.x) return;
-        const uint32_t xs = r.x - cb, xe = r.y - cb;  // wrap when r.x < cb: then out of the window
-        if (xs >= span || xe >= span) {
-          out = true;
-          return;
-        }
-        const uint32_t ws = xs >> 5, we = xe >> 5;
-        const uint32_t lo = ~0u << (xs & 31);
-        const uint32_t hi = ~0u >> (31 - (xe & 31));
-        top = max(top, we + 1);
-        bottom = min(bottom, ws);
-        if (ws == we) {
-          atomicOr(bits + ws, lo & hi);
-        } else {
-          atomicOr(bits + ws, lo);
-          atomicOr(bits + we, hi);
-          if (we > ws + 1) atomicMax(reach + ws + 1, we);
-        }
-      });
-      __syncwarp();
-      if (!__any_sync(kFullMask, out)) {
-        // words from the first to one past the last touched: runs close there
-        const uint32_t nw = min(uint32_t(kWWin), group_max<32>(kFullMask, top) + 1);
-        const uint32_t w_first = group_min<32>(kFullMask, bottom) & ~31u;  // below: empty words
-        uint64_t count = 0;
-        uint32_t carry = 0, run_reach = 0;
-        for (uint32_t wb = w_first; wb < nw; wb += 32) {
-          const uint32_t w = wb + lane;
-          const bool valid = w < nw;
-          uint32_t x = 0, rr = 0;
-          if (valid) {
-            x = bits[w];
-            rr = reach[w];
-          }
-          rr = group_incl_max<32>(kFullMask, rr, lane);
-          rr = max(rr, run_reach);
-          if (valid && rr > w) x = ~0u;
-          run_reach = __shfl_sync(kFullMask, rr, 31);
-          if (nnz) *nnz += __popc(x);
-          count += gather_chunk(x, valid, uint64_t(cb) + 32ull * w, 32, lane, kFullMask, carry, count,
-                                min(31u, nw - 1 - wb), emit);
-        }
-        __syncwarp();
-        return count;
-      }
-    }
-  }
-  // the general form: the row's column bounds first, then windows over them
-  uint32_t mn = 0xffffffffu, mx = 0;
-  wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
-    if (r.y < r.x) return;
-    mn = min(mn, r.x);
-    mx = max(mx, r.y);
-  });
-  mn = group_min<32>(kFullMask, mn);
-  mx = group_max<32>(kFullMask, mx);
-  if (mn > mx) return 0;
-  uint64_t count = 0;
-  const uint64_t base = mn & ~31u;
-  const uint64_t nw_total = ((uint64_t(mx) - base) >> 5) + 2;
-  uint32_t carry = 0;
-  for (uint64_t w0 = 0; w0 < nw_total; w0 += kWWin) {
-    const uint32_t nwc = uint32_t(min(uint64_t(kWWin), nw_total - w0));
-    const uint64_t cb = base + 32 * w0;
-    const uint64_t ce = cb + 32ull * nwc - 1;
-    for (uint32_t w = lane; w < nwc; w += 32) {
-      bits[w] = 0;
-      reach[w] = 0;
-    }
-    __syncwarp();
-    wide_ranges(p, row, a0, a1, d0, d1, b0, b1, [&](uint2 r) {
-      const uint64_t cs = max(uint64_t(r.x), cb);
-      const uint64_t cf = min(uint64_t(r.y), ce);
-      if (cs > cf || r.y < r.x) return;
-      const uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
-      const uint32_t lo = ~0u << (cs & 31);
-      const uint32_t hi = ~0u >> (31 - (cf & 31));
-      if (ws == we) {
-        atomicOr(bits + ws, lo & hi);
-      } else {
-        atomicOr(bits + ws, lo);
-        atomicOr(bits + we, hi);
-        if (we > ws + 1) atomicMax(reach + ws + 1, we);
-      }
-    });
-    __syncwarp();
-    uint32_t run_reach = 0;
-    for (uint32_t wb = 0; wb < nwc; wb += 32) {
-      const uint32_t w = wb + lane;
-      const bool valid = w < nwc;
-      uint32_t x = 0, rr = 0;
-      if (valid) {
-        x = bits[w];
-        rr = reach[w];
-      }
-      rr = group_incl_max<32>(kFullMask, rr, lane);
-      rr = max(rr, run_reach);
-      if (valid && rr > w) x = ~0u;
-      run_reach = __shfl_sync(kFullMask, rr, 31);
-      if (nnz) *nnz += __popc(x);
-      const uint32_t last = min(31u, nwc - 1 - wb);
-      count += gather_chunk(x, valid, cb + 32ull * w, 32, lane, kFullMask, carry, count, last, emit);
-    }
-    __syncwarp();
-  }
-  return count;
-}
-
 // Warp 0 walks back from chunk t (its aggregate published) to the nearest
 // inclusive prefix, publishes t's inclusive prefix (and, for the last chunk,
 // the product's total, with the overflow check) and leaves t's exclusive
@@ -323,7 +132,7 @@ __global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
       uint32_t bpos = 0;
       for (uint32_t r = warp; r < crows; r += kWWarps) {
         const uint32_t start = bpos;
-        const uint64_t c = wide_row(p, uint64_t(c0) + r, bits, reach, &nnz_acc, [&](uint64_t k, uint32_t v) {
+        const uint64_t c = wide_row<kWWin>(p, uint64_t(c0) + r, bits, reach, &nnz_acc, [&](uint64_t k, uint32_t v) {
           if (start + k < uint64_t(kWBuf)) buf[start + k] = v;
         });
         const bool kept = start + c <= uint64_t(kWBuf);
@@ -371,7 +180,7 @@ __global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
             bp += n;
           } else {
             bool bad = false;
-            const uint64_t c = wide_row(p, uint64_t(c0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
+            const uint64_t c = wide_row<kWWin>(p, uint64_t(c0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
               if (k < n) img[o + k] = v;
               else bad = true;
             });
@@ -416,7 +225,7 @@ __global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
         } else if (n) {
           uint32_t* dst = p.c_entries + prefix + o;
           bool bad = false;
-          const uint64_t c = wide_row(p, uint64_t(c0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
+          const uint64_t c = wide_row<kWWin>(p, uint64_t(c0) + r, bits, reach, nullptr, [&](uint64_t k, uint32_t v) {
             if (k < n) dst[k] = v;
             else bad = true;
           });
