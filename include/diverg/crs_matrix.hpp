@@ -9,8 +9,10 @@
  *  Storage is the same pair of std::vectors (entries: flattened inclusive
  *  [start, end] column ranges; rowmap: entry offsets, two per range), so the
  *  host-side behaviour and the on-disk bytes are those of the reference.
- *  Only the RangeDynamic spec with uint32_t columns is provided: the B200 path
- *  computes on it.
+ *  The B200 path computes on the RangeDynamic spec with uint32_t columns.
+ *  CRSMatrix< crs_matrix::RangeCompressed, ... > (crs_matrix.hpp:1050-1133,
+ *  :2245-2386 there) stores a built matrix immutably as Elias-delta coded
+ *  entries and rowmap (diverg/enc_vector.hpp) and answers the same queries.
  */
 #ifndef DIVERG_B200_CRS_MATRIX_HPP__
 #define DIVERG_B200_CRS_MATRIX_HPP__
@@ -23,9 +25,12 @@
 #include <utility>
 #include <vector>
 
+#include "diverg/enc_vector.hpp"
+
 namespace diverg {
   namespace crs_matrix {
     struct RangeDynamic { };
+    struct RangeCompressed { };
     struct RangeGroup { };
     struct BasicGroup { };
 
@@ -182,10 +187,123 @@ namespace diverg {
     rowmap_type rowmap;
   };
 
+  /** The immutable, compressed form of a range-CRS matrix: entries and rowmap
+   *  Elias-delta coded (crs_matrix.hpp:1050-1133: sdsl::enc_vector over
+   *  elias_delta), built from a RangeDynamic matrix and read with the same
+   *  queries (crs_matrix.hpp:2245-2386).  A row's entries are decoded from the
+   *  nearest sample before them; modifying the matrix is not offered, as in
+   *  the reference ("A Compressed Range CRS cannot be modified"). */
+  template< typename TOrdinal, typename TSize >
+  class CRSMatrix< crs_matrix::RangeCompressed, bool, TOrdinal, TSize > {
+    static_assert( std::is_same< TOrdinal, uint32_t >::value, "the B200 path uses uint32_t columns" );
+
+  public:
+    typedef crs_matrix::RangeCompressed spec_type;
+    typedef bool value_type;
+    typedef TOrdinal ordinal_type;
+    typedef TSize size_type;
+    typedef EliasDeltaVector entries_type;
+    typedef EliasDeltaVector rowmap_type;
+    typedef CRSMatrix< crs_matrix::RangeDynamic, bool, TOrdinal, TSize > mutable_type;
+
+    CRSMatrix( ) : num_cols( 0 ), m_nnz( 0 ), rowmap( std::vector< uint64_t >( 1, 0 ) ) { }
+
+    /** Compresses a built matrix (crs_matrix.hpp:2263-2270: by way of the mutable spec). */
+    explicit CRSMatrix( mutable_type const& m )
+      : num_cols( m.numCols() ), m_nnz( m.nnz() ), entries( m.get_entries() ), rowmap( m.get_rowmap() )
+    { }
+
+    inline ordinal_type numCols( ) const { return this->num_cols; }
+    inline ordinal_type numRows( ) const { return static_cast< ordinal_type >( this->rowmap.size() - 1 ); }
+    inline size_type nnz( ) const { return this->m_nnz; }
+    inline size_type rowMap( ordinal_type i ) const { return static_cast< size_type >( this->rowmap[ i ] ); }
+    inline ordinal_type entry( size_type k ) const { return static_cast< ordinal_type >( this->entries[ k ] ); }
+
+    /** Row i's flattened ranges. */
+    inline std::vector< ordinal_type >
+    row( ordinal_type i ) const
+    {
+      std::vector< ordinal_type > out;
+      this->entries.decode( this->rowMap( i ), this->rowMap( i + 1 ), out );
+      return out;
+    }
+
+    /** crs_matrix.hpp:1197-1218 over the decoded row. */
+    inline value_type
+    operator()( ordinal_type i, ordinal_type j ) const
+    {
+      const std::vector< ordinal_type > r = this->row( i );
+      return crs_matrix::binary_search( r.begin(), r.end(), j, crs_matrix::RangeGroup{} );
+    }
+
+    inline value_type
+    at( ordinal_type i, ordinal_type j ) const
+    {
+      if ( i >= this->numRows() || j >= this->numCols() ) throw std::runtime_error( "index out of range" );
+      return ( *this )( i, j );
+    }
+
+    /** crs_matrix.hpp:1127-1132: the coded vectors and the two scalars. */
+    inline size_type
+    size_in_bytes( ) const
+    {
+      return static_cast< size_type >( this->entries.size_in_bytes() + this->rowmap.size_in_bytes()
+                                       + sizeof( TOrdinal ) + sizeof( TSize ) );
+    }
+
+    /** The matrix decoded back into its mutable form. */
+    inline mutable_type
+    decompress( ) const
+    {
+      typename mutable_type::entries_type e;
+      typename mutable_type::rowmap_type r;
+      this->entries.decode( 0, this->entries.size(), e );
+      this->rowmap.decode( 0, this->rowmap.size(), r );
+      return mutable_type( this->num_cols, std::move( e ), std::move( r ), this->m_nnz );
+    }
+
+    /** The two coded vectors (entries, then rowmap), then ncols and nnz as
+     *  uint64, in the order of crs_matrix.hpp:1392-1409 and :1986-2000; the
+     *  coded vectors are this library's own layout, not sdsl's. */
+    inline void
+    serialize( std::ostream& out ) const
+    {
+      this->entries.serialize( out );
+      this->rowmap.serialize( out );
+      const uint64_t nc = this->num_cols, nz = this->m_nnz;
+      out.write( reinterpret_cast< const char* >( &nc ), sizeof( nc ) );
+      out.write( reinterpret_cast< const char* >( &nz ), sizeof( nz ) );
+    }
+
+    inline void
+    load( std::istream& in )
+    {
+      this->entries.load( in );
+      this->rowmap.load( in );
+      uint64_t nc = 0, nz = 0;
+      in.read( reinterpret_cast< char* >( &nc ), sizeof( nc ) );
+      in.read( reinterpret_cast< char* >( &nz ), sizeof( nz ) );
+      if ( !in || this->rowmap.size() == 0 ) throw std::runtime_error( "RangeCompressed: malformed stream" );
+      this->num_cols = static_cast< ordinal_type >( nc );
+      this->m_nnz = static_cast< size_type >( nz );
+    }
+
+  private:
+    ordinal_type num_cols;
+    size_type m_nnz;
+    entries_type entries;
+    rowmap_type rowmap;
+  };
+
+  template< typename TOrdinal = uint32_t, typename TSize = uint64_t >
+  using RangeCompressedCRSMatrix = CRSMatrix< crs_matrix::RangeCompressed, bool, TOrdinal, TSize >;
+
   namespace crs_matrix {
     template< typename T > struct is_range_crs_matrix : std::false_type { };
     template< typename TOrdinal, typename TSize >
     struct is_range_crs_matrix< CRSMatrix< RangeDynamic, bool, TOrdinal, TSize > > : std::true_type { };
+    template< typename TOrdinal, typename TSize >
+    struct is_range_crs_matrix< CRSMatrix< RangeCompressed, bool, TOrdinal, TSize > > : std::true_type { };
   }  // namespace crs_matrix
 }  // namespace diverg
 
