@@ -50,6 +50,7 @@ L2_BYTES = 126 * 2**20
 ROWMODE_TRAFFIC_BYTES_PER_ROW = (487831040 + 323487744 + 326833408 +
                                  154045184 + 137517312 + 142550272) / 3 / 10019292
 QUERY_ALG_BYTES = 33  # pair 8 B, two rowmap words 16 B, one range 8 B, answer 1 B
+QUERY_SECTOR_BYTES = 73  # two 32-byte sectors (row pointers, range), the pair, the answer
 
 
 def parse_args():
@@ -282,7 +283,13 @@ def run_query(args, ctx, stream, d_idx, a, want, npairs=1_000_000, steps=20, war
             "call_us": call_s * 1e6,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "alg_bytes_per_query": QUERY_ALG_BYTES,
-                         "note": "random rows: every pair touches at least two 32-byte DRAM sectors (rowmap, range)"},
+                         # a random pair moves whole 32-byte sectors: its row's two
+                         # pointers and its range (one sector each at least), its
+                         # 8-byte pair and its answer byte
+                         "sector_bytes_per_query": QUERY_SECTOR_BYTES,
+                         "frac_of_sector_bound": ach / peak * QUERY_SECTOR_BYTES / QUERY_ALG_BYTES,
+                         "note": "random rows: every pair touches at least two 32-byte DRAM sectors (rowmap, "
+                                 "range), so the 33-byte algorithmic count caps frac at 33/73 of peak"},
             "e2e": {"value": npairs / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(h_pairs.nbytes),
                     "d2h_bytes_per_step": int(npairs), "note": "pageable host buffers, one call"},
             "answers_in_range": int(got.sum()), "parity": parity,
