@@ -31,9 +31,20 @@
 namespace dvg {
 namespace {
 
-constexpr int kWThreads = 256;
+#ifndef DVG_WIDE_THREADS
+#define DVG_WIDE_THREADS 256
+#endif
+#ifndef DVG_WIDE_ROWS
+#define DVG_WIDE_ROWS 128
+#endif
+#ifndef DVG_WIDE_MINB
+#define DVG_WIDE_MINB 4
+#endif
+constexpr int kWThreads = DVG_WIDE_THREADS;
 constexpr int kWWarps = kWThreads / 32;
-constexpr int kWRows = 64;     // rows of a chunk
+constexpr int kWRows = DVG_WIDE_ROWS;  // rows of a chunk
+constexpr int kWRowsLane = kWRows / 32;  // rows of the chunk prefix a lane sums
+static_assert(kWRows % 32 == 0 && kWRowsLane >= 1, "chunk rows are a multiple of 32");
 constexpr int kWWin = 128;     // window words of a warp (4,096 columns)
 constexpr int kWBuf = 256;     // run entries of a warp's rows kept from the count
 constexpr int kWImage = 2048;  // output entries of a chunk held for its deferred write-out
@@ -109,7 +120,7 @@ __device__ void wide_lookback(unsigned long long* out, const FusedArgs& p, uint3
   }
 }
 
-__global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
+__global__ void __launch_bounds__(kWThreads, DVG_WIDE_MINB) k_spgemm_wide(FusedArgs p) {
   extern __shared__ __align__(16) unsigned char wide_smem_raw[];
   WideSmem& S = *reinterpret_cast<WideSmem*>(wide_smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -144,11 +155,17 @@ __global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
         if (kept) bpos += uint32_t(c);
       }
       wide_sync();
-      // 2. chunk-local prefix (warp 0: two rows a lane)
+      // 2. chunk-local prefix (warp 0: kWRowsLane consecutive rows a lane)
       if (warp == 0) {
-        const uint32_t r0 = 2 * lane, r1 = 2 * lane + 1;
-        const uint32_t v0 = r0 < crows ? S.cnt_row[r0] : 0u, v1 = r1 < crows ? S.cnt_row[r1] : 0u;
-        uint64_t incl = uint64_t(v0) + v1;
+        uint32_t v[kWRowsLane];
+        uint64_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < kWRowsLane; ++k) {
+          const uint32_t r = kWRowsLane * lane + k;
+          v[k] = r < crows ? S.cnt_row[r] : 0u;
+          sum += v[k];
+        }
+        uint64_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const uint64_t u = __shfl_up_sync(kFullMask, incl, o);
@@ -158,8 +175,13 @@ __global__ void __launch_bounds__(kWThreads, 4) k_spgemm_wide(FusedArgs p) {
         if (total > 0xffffffffull) {
           if (lane == 0) raise_flag(p, &p.ctl->status, 16ull);
         }
-        if (r0 < crows) S.incl[b][r0] = uint32_t(incl - v1);
-        if (r1 < crows) S.incl[b][r1] = uint32_t(incl);
+        uint64_t run = incl - sum;
+#pragma unroll
+        for (int k = 0; k < kWRowsLane; ++k) {
+          const uint32_t r = kWRowsLane * lane + k;
+          run += v[k];
+          if (r < crows) S.incl[b][r] = uint32_t(run);
+        }
         if (lane == 0) {
           S.cnt = uint32_t(total);
           publish_aggregate(p, t, total);
