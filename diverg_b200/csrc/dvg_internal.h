@@ -40,6 +40,10 @@ struct DeviceControl {
   unsigned long long slow_rows;     // row-mode rows that missed the shared window
 };
 
+// DeviceControl::status bit of a query that met row pointers outside its
+// index's entries (the pair is answered 0, nothing past the entries is read).
+constexpr unsigned long long kQueryCorrupt = 128ull;
+
 // A row-kernel shape chosen by the autotuner.
 struct TuneChoice {
   int slot_variant;    // run-list entries per thread: 0 -> 16, 1 -> 24, 2 -> 32

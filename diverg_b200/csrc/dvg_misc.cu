@@ -524,15 +524,21 @@ __global__ void __launch_bounds__(kAddThreads) k_spadd_chunks(SpaddChunkArgs p) 
 // 149-169, one thread per pair ------------------------------------------------
 __global__ void __launch_bounds__(kThreads) k_query(const uint64_t* __restrict__ rowmap,
                                                     const uint32_t* __restrict__ entries, uint32_t nrows,
-                                                    uint32_t ncols, const uint2* __restrict__ pairs, uint64_t npairs,
+                                                    uint32_t ncols, uint64_t nentries,
+                                                    const uint2* __restrict__ pairs, uint64_t npairs,
                                                     uint8_t* __restrict__ out, DeviceControl* ctl) {
   unsigned long long bad = 0;
+  bool corrupt = false;
   for (uint64_t q = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; q < npairs;
        q += uint64_t(gridDim.x) * blockDim.x) {
     uint2 ij = pairs[q];
     uint8_t ans = 0;
     if (ij.x < nrows && ij.y < ncols) {
-      const uint64_t lo = __ldg(rowmap + ij.x), hi = __ldg(rowmap + ij.x + 1);
+      uint64_t lo = __ldg(rowmap + ij.x), hi = __ldg(rowmap + ij.x + 1);
+      if (lo > hi || hi > nentries) {  // row pointers outside the entries: never read past them
+        corrupt = true;
+        lo = hi = 0;
+      }
       uint64_t first = lo, len = hi - lo;
       while (len > 0) {
         uint64_t half = len >> 1;
@@ -551,6 +557,7 @@ __global__ void __launch_bounds__(kThreads) k_query(const uint64_t* __restrict__
     out[q] = ans;
   }
   if (bad) atomicAdd(&ctl->invalid, bad);
+  if (corrupt) atomicOr(&ctl->status, kQueryCorrupt);
 }
 
 // Four consecutive pairs a thread, their loads interleaved: the pairs (two
@@ -565,9 +572,11 @@ __device__ __forceinline__ uint32_t pick4(uint2 e0, uint2 e1, uint64_t k) {
 
 __global__ void __launch_bounds__(kThreads) k_query4(const uint64_t* __restrict__ rowmap,
                                                      const uint32_t* __restrict__ entries, uint32_t nrows,
-                                                     uint32_t ncols, const uint4* __restrict__ pairs, uint64_t ngroups,
+                                                     uint32_t ncols, uint64_t nentries,
+                                                     const uint4* __restrict__ pairs, uint64_t ngroups,
                                                      uchar4* __restrict__ out, DeviceControl* ctl) {
   unsigned long long bad = 0;
+  bool corrupt = false;
   for (uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; g < ngroups;
        g += uint64_t(gridDim.x) * blockDim.x) {
     const uint4 p01 = __ldg(pairs + 2 * g), p23 = __ldg(pairs + 2 * g + 1);
@@ -580,6 +589,10 @@ __global__ void __launch_bounds__(kThreads) k_query4(const uint64_t* __restrict_
       bad += ok[k] ? 0 : 1;
       lo[k] = ok[k] ? __ldg(rowmap + qi[k]) : 0;
       hi[k] = ok[k] ? __ldg(rowmap + qi[k] + 1) : 0;
+      if (lo[k] > hi[k] || hi[k] > nentries) {  // row pointers outside the entries: never read past them
+        corrupt = true;
+        lo[k] = hi[k] = 0;
+      }
     }
     uint2 e0[4], e1[4];
 #pragma unroll
@@ -628,6 +641,7 @@ __global__ void __launch_bounds__(kThreads) k_query4(const uint64_t* __restrict_
     out[g] = make_uchar4(ans[0], ans[1], ans[2], ans[3]);
   }
   if (bad) atomicAdd(&ctl->invalid, bad);
+  if (corrupt) atomicOr(&ctl->status, kQueryCorrupt);
 }
 
 }  // namespace
@@ -756,7 +770,7 @@ void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pai
   if (vec && npairs >= 4) {
     const uint64_t groups = npairs / 4;
     k_query4<<<grid_for(ctx, groups, kThreads, 8), kThreads, 0, ctx->stream>>>(
-        idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint4*>(d_pairs), groups,
+        idx->rowmap, idx->entries, idx->nrows, idx->ncols, idx->nentries, reinterpret_cast<const uint4*>(d_pairs), groups,
         reinterpret_cast<uchar4*>(d_out), c);
     DVG_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
@@ -764,7 +778,7 @@ void launch_query(dvg_context* ctx, const dvg_matrix* idx, const uint32_t* d_pai
   }
   if (done < npairs) {
     k_query<<<grid_for(ctx, npairs - done, kThreads, 16), kThreads, 0, ctx->stream>>>(
-        idx->rowmap, idx->entries, idx->nrows, idx->ncols, reinterpret_cast<const uint2*>(d_pairs) + done,
+        idx->rowmap, idx->entries, idx->nrows, idx->ncols, idx->nentries, reinterpret_cast<const uint2*>(d_pairs) + done,
         npairs - done, d_out + done, c);
     DVG_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;

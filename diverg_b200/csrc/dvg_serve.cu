@@ -258,6 +258,24 @@ void build_worker(dvg_server* s, size_t w) {
         }
       }
     }
+    // the indices are read on the query context's stream from here on: the
+    // last kernels that write them (the batch's split, an exact-size copy)
+    // are still queued on this stream when the build returns, so wait for them
+    {
+      const uint64_t ts = now();
+      const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+      ctx->stats.host_sync_ns += now() - ts;
+      ctx->stats.host_syncs++;
+      if (e != cudaSuccess) {
+        for (size_t k = 0; k < nb; ++k) {
+          if (status[k] == DVG_OK) {
+            status[k] = DVG_ERR_DEVICE;
+            why[k] = std::string("build batch: ") + cudaGetErrorString(e);
+          }
+          out[k] = nullptr;  // never published; the context is unusable after a device error
+        }
+      }
+    }
     for (dvg_matrix* m : in)
       if (m) dvg::free_matrix(ctx, m);
     const uint64_t t_done = now();
@@ -386,6 +404,10 @@ void query_worker(dvg_server* s) {
         dvg::record_error(std::string("query batch: ") + cudaGetErrorString(e));
       }
       if (status == DVG_OK && q.staged_out) std::memcpy(q.req.answers, q.h_out, q.req.npairs);
+      if (status == DVG_OK && q.h_ctl->status) {
+        status = DVG_ERR_DEVICE;
+        dvg::record_error("query batch: the index's row pointers lie outside its entries");
+      }
       const uint64_t invalid = status == DVG_OK ? q.h_ctl->invalid : 0;
       std::lock_guard<std::mutex> lk(s->mu);
       auto f = s->indices.find(q.req.index);

@@ -548,3 +548,35 @@ def test_query_out_of_range_pairs_answer_zero_in_both_paths(ctx):
         ctx.query_device(d, d_pairs.data_ptr(), len(pairs), d_out.data_ptr())
     torch.cuda.synchronize()
     assert np.array_equal(d_out.cpu().numpy(), want)
+
+
+def test_query_never_reads_past_a_corrupt_index(ctx):
+    # row pointers that leave the entries (a caller-owned index overwritten
+    # after it was wrapped): those pairs answer 0, nothing past the entries is
+    # read, the call reports a device error and the context stays usable
+    import torch
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(20_000, seed=333))
+    n = a.numRows()
+    rowmap = torch.from_numpy(a.rowmap.astype(np.uint64).view(np.int64)).cuda()
+    entries = torch.from_numpy(a.entries.view(np.int32)).cuda()
+    d = ctx.wrap_device(n, a.numCols(), rowmap.data_ptr(), entries.data_ptr(), len(a.entries), a.nnz())
+    pairs = np.array([[k, k + 1] for k in range(64)], np.uint32)
+    want = orc.query(omat(a), pairs)
+    assert np.array_equal(ctx.query(d, pairs), want)
+    rowmap[10] = 1 << 40   # row 9 ends and row 10 starts far past the entries
+    rowmap[20] = -1        # row 19 ends and row 20 starts at 2^64 - 1
+    torch.cuda.synchronize()
+    npairs = len(pairs)
+    bad = np.isin(np.arange(npairs), [9, 10, 19, 20])
+    for offset in (0, 1):  # the four-pair kernel; buffers offset by a pair: the one-pair kernel
+        padded = np.concatenate([np.zeros((offset, 2), np.uint32), pairs])
+        d_pairs = torch.from_numpy(padded.view(np.int32).reshape(-1)).cuda()
+        d_out = torch.full((npairs + offset,), 7, dtype=torch.uint8, device="cuda")
+        with pytest.raises(N.DvgError) as err:
+            ctx.query_device(d, d_pairs.data_ptr() + 8 * offset, npairs, d_out.data_ptr() + offset)
+        assert err.value.status == N.DEVICE
+        got = d_out.cpu().numpy()[offset:]
+        assert (got[bad] == 0).all() and np.array_equal(got[~bad], want[~bad])
+    rowmap.copy_(torch.from_numpy(a.rowmap.astype(np.uint64).view(np.int64)).cuda())
+    torch.cuda.synchronize()
+    assert np.array_equal(ctx.query(d, pairs), want)

@@ -161,3 +161,20 @@ def test_builds_run_side_by_side_on_two_workers():
         for g, b in ((long_g, bl), (short_g, bs)):
             want = orc.dindex(omat(g), *WINDOW, algo="hbv")
             assert same(srv.download(b), CRSMatrix(want.ncols, want.entries, want.rowmap, want.nnz))
+
+
+def test_queries_waiting_on_a_build_read_the_finished_index():
+    # every query is submitted right behind the build of its index, so it is
+    # issued (on the query stream) the moment the build completes: it must see
+    # the whole index, as the same pairs against the downloaded index do
+    graphs = [graph(int(n), seed=600 + k) for k, n in enumerate(np.linspace(3_000, 60_000, 16))]
+    pairs = [gen.query_pairs(g, 20_000, 0.5, *WINDOW, seed=700 + k) for k, g in enumerate(graphs)]
+    with Server(device=0, max_batch_builds=2, max_inflight_queries=8) as srv:
+        bids, qids, answers = [], [], []
+        for k, g in enumerate(graphs):
+            bids.append(srv.submit_build(g, *WINDOW))
+            answers.append(np.full(len(pairs[k]), 7, np.uint8))
+            qids.append(srv.submit_query(bids[k], pairs[k], answers[k]))
+        assert all(c["status"] == N.OK for c in srv.wait(bids + qids))
+        for k in range(len(graphs)):
+            assert np.array_equal(answers[k], orc.query(omat(srv.download(bids[k])), pairs[k])), k
