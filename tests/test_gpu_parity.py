@@ -480,12 +480,14 @@ def _noncanonical(m, split_every=1):
 
 
 @pytest.mark.parametrize("single", [1, 0])
-@pytest.mark.parametrize("shape", ["banded", "wide_rows", "noncanonical", "empty_rows", "one_row"])
+@pytest.mark.parametrize("shape", ["banded", "wide_rows", "noncanonical", "empty_rows", "one_row", "dense_disjoint",
+                                   "cover"])
 def test_spadd_one_pass_and_three_pass(ctx, single, shape):
     # range_spadd (range_sparse.hpp:112-477) in one pass with a chunk look-back
     # and by count, scan and fill: rows past the per-chunk stages (wide rows),
-    # chunks whose output exceeds the shared image, the reference's merge on
-    # non-canonical rows (tails copied verbatim), empty rows
+    # chunks whose output exceeds the shared image (dense, disjoint), long
+    # ranges of one operand covering many of the other's (cover), the
+    # reference's merge on non-canonical rows (tails copied verbatim), empty rows
     if shape == "banded":
         a = gen.banded(300_000, 512, 4.0, 32.0, seed=301)
         b = gen.banded(300_000, 512, 4.0, 32.0, seed=302)
@@ -498,6 +500,12 @@ def test_spadd_one_pass_and_three_pass(ctx, single, shape):
     elif shape == "empty_rows":
         a = gen.random_matrix(50_000, 5_000, seed=307)
         b = gen.random_matrix(50_000, 3_000, seed=308)
+    elif shape == "dense_disjoint":
+        a = gen.banded(40_000, 4000, 5.0, 1.5, seed=309)
+        b = gen.banded(40_000, 4000, 5.0, 1.5, seed=310)
+    elif shape == "cover":
+        a = gen.banded(50_000, 512, 5.0, 3.0, seed=311)
+        b = gen.banded(50_000, 512, 0.5, 600.0, seed=312)
     else:
         a = CRSMatrix(9, np.array([0, 3, 5, 8], np.uint32), np.array([0, 4], np.uint64))
         b = CRSMatrix(9, np.array([4, 4], np.uint32), np.array([0, 2], np.uint64))
