@@ -561,6 +561,24 @@ __device__ uint32_t light_row(const uint32_t* crow, const uint2* achunk, const F
 
 // ---- warp path for rows that name many B ranges ------------------------------
 
+// Window word w of the calling lane (32 consecutive words a warp) and its
+// reach rr (one past the largest end column, in window columns, of the
+// ranges that start in word w and end past it; 0: none): the bits of word w
+// that ranges starting in earlier words cover -- everything from the word's
+// first column to the largest reach before it.  run_reach carries the largest
+// reach of the earlier 32-word blocks and is advanced past this block.
+__device__ __forceinline__ uint32_t reach_cover(uint32_t w, uint32_t rr, uint32_t& run_reach, int lane) {
+  const uint32_t incl = group_incl_max<32>(kFullMask, rr, lane);
+  uint32_t before = __shfl_up_sync(kFullMask, incl, 1);
+  before = max(lane ? before : 0u, run_reach);
+  run_reach = max(run_reach, __shfl_sync(kFullMask, incl, 31));
+  const uint32_t c0 = 32u * w;  // the word's first column
+  if (before <= c0) return 0u;
+  const uint32_t n = before - c0;  // covered columns from c0
+  return n >= 32u ? ~0u : (1u << n) - 1u;
+}
+
+
 // Calls f(range) on this lane's share of the addend's ranges of `row` and of
 // every B range the row's A ranges name.  The slice bounds of the first 32 A
 // ranges are loaded once (by the lanes, together) and kept in b0 / b1.
@@ -658,13 +676,11 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
         const uint32_t hi = ~0u >> (31 - (xe & 31));
         top = max(top, we + 1);
         bottom = min(bottom, ws);
-        if (ws == we) {
-          atomicOr(bits + ws, lo & hi);
-        } else {
-          atomicOr(bits + ws, lo);
-          atomicOr(bits + we, hi);
-          if (we > ws + 1) atomicMax(reach + ws + 1, we);
-        }
+        // the range's bits in its first word; past that word, its end column
+        // (+ 1) as that word's reach: later words are covered up to the
+        // largest reach of the words before them
+        atomicOr(bits + ws, ws == we ? lo & hi : lo);
+        if (ws != we) atomicMax(reach + ws, xe + 1u);
       });
       __syncwarp();
       if (!__any_sync(kFullMask, out)) {
@@ -681,10 +697,8 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
             x = bits[w];
             rr = reach[w];
           }
-          rr = group_incl_max<32>(kFullMask, rr, lane);
-          rr = max(rr, run_reach);
-          if (valid && rr > w) x = ~0u;
-          run_reach = __shfl_sync(kFullMask, rr, 31);
+          const uint32_t cov = reach_cover(w, rr, run_reach, lane);
+          if (valid) x |= cov;
           if (nnz) *nnz += __popc(x);
           count += gather_chunk(x, valid, uint64_t(cb) + 32ull * w, 32, lane, kFullMask, carry, count,
                                 min(31u, nw - 1 - wb), emit);
@@ -724,13 +738,8 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
       const uint32_t ws = uint32_t((cs - cb) >> 5), we = uint32_t((cf - cb) >> 5);
       const uint32_t lo = ~0u << (cs & 31);
       const uint32_t hi = ~0u >> (31 - (cf & 31));
-      if (ws == we) {
-        atomicOr(bits + ws, lo & hi);
-      } else {
-        atomicOr(bits + ws, lo);
-        atomicOr(bits + we, hi);
-        if (we > ws + 1) atomicMax(reach + ws + 1, we);
-      }
+      atomicOr(bits + ws, ws == we ? lo & hi : lo);
+      if (ws != we) atomicMax(reach + ws, uint32_t(cf - cb) + 1u);
     });
     __syncwarp();
     uint32_t run_reach = 0;
@@ -742,10 +751,8 @@ __device__ uint64_t wide_row(const FusedArgs& p, uint64_t row, uint32_t* bits, u
         x = bits[w];
         rr = reach[w];
       }
-      rr = group_incl_max<32>(kFullMask, rr, lane);
-      rr = max(rr, run_reach);
-      if (valid && rr > w) x = ~0u;
-      run_reach = __shfl_sync(kFullMask, rr, 31);
+      const uint32_t cov = reach_cover(w, rr, run_reach, lane);
+      if (valid) x |= cov;
       if (nnz) *nnz += __popc(x);
       const uint32_t last = min(31u, nwc - 1 - wb);
       count += gather_chunk(x, valid, cb + 32ull * w, 32, lane, kFullMask, carry, count, last, emit);
