@@ -366,13 +366,8 @@ __global__ void __launch_bounds__(kWThreads, 4) k_rangeop_calibrate(const uint2*
         const uint32_t lo = ~0u << (r.x & 31);
         const uint32_t hi = ~0u >> (31 - (r.y & 31));
         top = max(top, we + 1);
-        if (ws == we) {
-          atomicOr(bits + ws, lo & hi);
-        } else {
-          atomicOr(bits + ws, lo);
-          atomicOr(bits + we, hi);
-          if (we > ws + 1) atomicMax(reach + ws + 1, we);
-        }
+        atomicOr(bits + ws, ws == we ? lo & hi : lo);
+        if (ws != we) atomicMax(reach + ws, r.y + 1u);
       }
     }
     __syncwarp();
@@ -387,10 +382,8 @@ __global__ void __launch_bounds__(kWThreads, 4) k_rangeop_calibrate(const uint2*
         x = bits[w];
         rr = reach[w];
       }
-      rr = group_incl_max<32>(kFullMask, rr, lane);
-      rr = max(rr, run_reach);
-      if (valid && rr > w) x = ~0u;
-      run_reach = __shfl_sync(kFullMask, rr, 31);
+      const uint32_t cov = reach_cover(w, rr, run_reach, lane);
+      if (valid) x |= cov;
       nnz += __popc(x);
       count += gather_chunk(x, valid, 32ull * w, 32, lane, kFullMask, carry, count, min(31u, nw - 1 - wb),
                             [](uint64_t, uint32_t) {});
