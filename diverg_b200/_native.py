@@ -108,6 +108,7 @@ DVG_SIGNATURES = {
     "dvg_adjacency_from_graph": [_P, _U32, _P, ctypes.c_uint64, _P, _U32, _U32, _PP],
     "dvg_selftest_bounded_wait": [_P, _U32],
     "dvg_calibrate_range_ops": [_P, ctypes.POINTER(ctypes.c_double)],
+    "dvg_calibrate_random_reads": [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)],
     "dvg_query_batch": [_P, _P, _P, _U64, _P],
     "dvg_query_batch_host": [_P, _P, _P, _U64, _P],
     "dvg_range_spgemm_noalloc": [_U32, _U32, _P, _P, _U64, _U32, _U32, _P, _P, _U64, _P, _P, _U64,

@@ -1067,6 +1067,15 @@ dvg_status dvg_calibrate_range_ops(dvg_context* ctx, double* ops_per_second) {
   });
 }
 
+dvg_status dvg_calibrate_random_reads(dvg_context* ctx, uint64_t bytes, double* reads_per_second) {
+  return guarded([&] {
+    require(ctx != nullptr && reads_per_second != nullptr, "null argument");
+    require(bytes <= (uint64_t(1) << 40), "calibrate_random_reads: bytes above 2^40");
+    Lock lk(ctx);
+    *reads_per_second = calibrate_random_reads(ctx, bytes);
+  });
+}
+
 dvg_status dvg_adjacency_from_graph(dvg_context* ctx, uint32_t nnodes, const uint32_t* node_len, uint64_t nedges,
                                     const uint32_t* edges, uint32_t lower, uint32_t upper, dvg_matrix** out) {
   return guarded([&] {

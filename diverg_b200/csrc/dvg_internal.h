@@ -185,6 +185,8 @@ void launch_spgemm_wide(dvg_context* ctx, const dvg_matrix* a, const dvg_matrix*
 // Range operations a second the warp-per-row kernel's inner work sustains on
 // this device (measured; synchronises the context's stream).
 double calibrate_range_ops(dvg_context* ctx);
+// Random 8-byte reads a second over a buffer of `bytes` (dvg_misc.cu).
+double calibrate_random_reads(dvg_context* ctx, uint64_t bytes);
 void launch_row_shifted_sum(dvg_context* ctx, const dvg_matrix* u, uint32_t shift, uint64_t* c_rowmap,
                             uint32_t* c_entries, uint64_t cap);
 

@@ -644,7 +644,74 @@ __global__ void __launch_bounds__(kThreads) k_query4(const uint64_t* __restrict_
   if (corrupt) atomicOr(&ctl->status, kQueryCorrupt);
 }
 
+// ---- random reads: the denominator of the query's roofline -------------------
+// Independent 8-byte reads at uniformly random word addresses of a buffer,
+// kRandReads a thread in flight at once: each touches one DRAM sector, as a
+// membership query's row-pointer and range reads do.  Addresses are
+// SplitMix64 (Steele, Lea and Flood) of the read's index, scaled into
+// [0, nwords) by the high half of a 64 x 64-bit product.
+constexpr int kRandReads = 16;
+
+__global__ void __launch_bounds__(kThreads) k_random_reads(const uint64_t* __restrict__ buf, uint64_t nwords,
+                                                           uint64_t nthreads, unsigned long long* sink) {
+  uint64_t acc = 0;
+  for (uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; g < nthreads;
+       g += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t v[kRandReads];
+#pragma unroll
+    for (int k = 0; k < kRandReads; ++k) {
+      uint64_t z = (g * kRandReads + uint64_t(k) + 1) * 0x9E3779B97F4A7C15ull;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z ^= z >> 31;
+      v[k] = __ldg(buf + __umul64hi(z, nwords));
+    }
+#pragma unroll
+    for (int k = 0; k < kRandReads; ++k) acc ^= v[k];
+  }
+  // keeps the reads observable: one atomic a warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc ^= __shfl_xor_sync(kFullMask, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicXor(sink, acc);
+}
+
 }  // namespace
+
+double calibrate_random_reads(dvg_context* ctx, uint64_t bytes) {
+  const uint64_t nwords = std::max<uint64_t>(bytes / 8, 1u << 20);
+  const uint64_t nthreads = uint64_t(1) << 22;  // 2^26 reads a launch
+  void* mem = dalloc(ctx, nwords * 8 + 256);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float best = 0.f;
+  try {
+    auto* buf = static_cast<uint64_t*>(mem);
+    auto* sink = reinterpret_cast<unsigned long long*>(static_cast<char*>(mem) + nwords * 8);
+    DVG_CUDA(cudaMemsetAsync(mem, 0, nwords * 8 + 8, ctx->stream));
+    DVG_CUDA(cudaEventCreate(&e0));
+    DVG_CUDA(cudaEventCreate(&e1));
+    const unsigned grid = grid_for(ctx, nthreads, kThreads);
+    for (int rep = 0; rep < 4; ++rep) {  // the first is a warm-up; the best of the rest
+      DVG_CUDA(cudaEventRecord(e0, ctx->stream));
+      k_random_reads<<<grid, kThreads, 0, ctx->stream>>>(buf, nwords, nthreads, sink);
+      DVG_CUDA(cudaGetLastError());
+      DVG_CUDA(cudaEventRecord(e1, ctx->stream));
+      DVG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      DVG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0 && (best == 0.f || ms < best)) best = ms;
+    }
+    ctx->stats.kernel_launches += 4;
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    dfree(ctx, mem);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(ctx, mem);
+  return best > 0.f ? double(nthreads) * kRandReads / (double(best) * 1e-3) : 0.0;
+}
 
 void launch_identity(dvg_context* ctx, dvg_matrix* out) {
   if (out->nrows == 0) {

@@ -66,6 +66,13 @@ class Context:
         N.check(N.lib().dvg_calibrate_range_ops(self.handle, ctypes.byref(v)))
         return v.value
 
+    def calibrate_random_reads(self, nbytes):
+        """Independent random 8-byte reads a second over a device buffer of
+        nbytes (the denominator of the membership query's roofline)."""
+        v = ctypes.c_double()
+        N.check(N.lib().dvg_calibrate_random_reads(self.handle, nbytes, ctypes.byref(v)))
+        return v.value
+
     # -- matrices ---------------------------------------------------------------
     def upload(self, m: CRSMatrix) -> "DeviceMatrix":
         L = N.lib()

@@ -200,6 +200,14 @@ dvg_status dvg_selftest_bounded_wait(dvg_context* ctx, uint32_t spin_limit);
  * stream. */
 dvg_status dvg_calibrate_range_ops(dvg_context* ctx, double* ops_per_second);
 
+/* No counterpart in the reference: a measurement for the roofline of the
+ * membership query, whose pairs read rows at random.  Times independent
+ * 8-byte reads at uniformly random addresses of a device buffer of `bytes`
+ * (at least 8 MiB; the size of the queried index gives the same DRAM and TLB
+ * behaviour), each touching one 32-byte sector, and stores the reads a second
+ * the device sustained.  Synchronises the context's stream. */
+dvg_status dvg_calibrate_random_reads(dvg_context* ctx, uint64_t bytes, double* reads_per_second);
+
 /* ---- adjacency construction: util::range_adjacency_matrix
  *      (adjacency.hpp:249-265) over util::adjacency_matrix (:170-228) and the
  *      Basic->Range conversion of crs_matrix::append (crs_matrix.hpp:197-242)

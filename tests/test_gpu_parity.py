@@ -588,3 +588,15 @@ def test_query_never_reads_past_a_corrupt_index(ctx):
     rowmap.copy_(torch.from_numpy(a.rowmap.astype(np.uint64).view(np.int64)).cuda())
     torch.cuda.synchronize()
     assert np.array_equal(ctx.query(d, pairs), want)
+
+
+def test_random_read_calibration(ctx):
+    # the query's measured denominator: positive and finite, an argument
+    # error for an absurd size, and the context answers correctly afterwards
+    rate = ctx.calibrate_random_reads(64 << 20)
+    assert np.isfinite(rate) and 1e8 < rate < 1e12, rate
+    with pytest.raises(N.DvgError):
+        ctx.calibrate_random_reads(1 << 41)
+    a, _ = gen.graph_adjacency(gen.small_graph_spec(20_000, seed=334))
+    pairs = np.array([[k, k + 1] for k in range(0, 2000, 7)], np.uint32)
+    assert np.array_equal(ctx.query(ctx.upload(a), pairs), orc.query(omat(a), pairs))
