@@ -275,7 +275,7 @@ constexpr uint32_t kAddSpinLimit = 1u << 22;
 struct AddSmem {
   uint2 a[kAddStage];
   uint2 b[kAddStage];
-  uint32_t img[2][kAddImage];             // images of the counted and the pending chunk
+  uint2 img[2][kAddImage / 2];            // images of the counted and the pending chunk (ranges)
   uint32_t incl[2][kAddThreads];          // their chunk-local inclusive row counts
   unsigned long long arow[kAddThreads + 1];  // the chunk's row pointers (entry offsets)
   unsigned long long brow[kAddThreads + 1];
@@ -453,10 +453,8 @@ __global__ void __launch_bounds__(kAddThreads) k_spadd_chunks(SpaddChunkArgs p) 
       if (imaged) {
         S.incl[b][r] = excl + cnt_r;
         if (has)
-          spadd_row(reinterpret_cast<const uint32_t*>(ap), 2ull * na, reinterpret_cast<const uint32_t*>(bp), 2ull * nb, [&, k = excl](uint32_t lo, uint32_t hi) mutable {
-            S.img[b][k] = lo;
-            S.img[b][k + 1] = hi;
-            k += 2;
+          spadd_row(reinterpret_cast<const uint32_t*>(ap), 2ull * na, reinterpret_cast<const uint32_t*>(bp), 2ull * nb, [&, k = excl / 2](uint32_t lo, uint32_t hi) mutable {
+            S.img[b][k++] = make_uint2(lo, hi);
           });
       }
     }
@@ -469,8 +467,8 @@ __global__ void __launch_bounds__(kAddThreads) k_spadd_chunks(SpaddChunkArgs p) 
       if (uint32_t(tid) < prow) p.c_rowmap[uint64_t(pt) * kAddThreads + tid + 1] = prefix + S.incl[b ^ 1u][tid];
       if (pt == 0 && tid == 0) p.c_rowmap[0] = 0;
       if (prefix + pcnt <= p.cap) {
-        uint32_t* dst = p.c_entries + prefix;
-        for (uint32_t k = tid; k < pcnt; k += kAddThreads) dst[k] = S.img[b ^ 1u][k];
+        uint2* dst = reinterpret_cast<uint2*>(p.c_entries + prefix);  // prefix is even: 8-byte aligned
+        for (uint32_t k = tid; k < pcnt / 2; k += kAddThreads) dst[k] = S.img[b ^ 1u][k];
       } else if (tid == 0 && pcnt) {
         atomicOr(&p.ctl->overflow, 1ull);
       }
