@@ -572,19 +572,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       }
       if (pend_t == 0 && tid == 0) p.c_rowmap[0] = 0;
       if (prefix + pend_cnt <= p.cap) {
-        uint32_t* dst = p.c_entries + prefix;
-        constexpr int kBatch = 8;
-        for (uint64_t k0 = 0; k0 < pend_cnt; k0 += uint64_t(kBatch) * kThreads) {
-          uint32_t v[kBatch];
+        // ranges of 8 bytes: images start 8-byte aligned (17 words a chunk row,
+        // chunks of a multiple of 32 rows) and prefix is even
+        uint2* dst = reinterpret_cast<uint2*>(p.c_entries + prefix);
+        const uint2* src = reinterpret_cast<const uint2*>(img);
+        const uint64_t npend = pend_cnt / 2;
+        constexpr int kBatch = 4;
+        for (uint64_t k0 = 0; k0 < npend; k0 += uint64_t(kBatch) * kThreads) {
+          uint2 v[kBatch];
 #pragma unroll
           for (int u = 0; u < kBatch; ++u) {
             const uint64_t k = k0 + tid + uint64_t(u) * kThreads;
-            v[u] = k < pend_cnt ? __ldcg(img + k) : 0u;
+            v[u] = k < npend ? __ldcg(src + k) : make_uint2(0u, 0u);
           }
 #pragma unroll
           for (int u = 0; u < kBatch; ++u) {
             const uint64_t k = k0 + tid + uint64_t(u) * kThreads;
-            if (k < pend_cnt) dst[k] = v[u];
+            if (k < npend) dst[k] = v[u];
           }
         }
       } else if (tid == 0 && pend_cnt) {
