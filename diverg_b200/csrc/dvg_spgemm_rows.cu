@@ -544,7 +544,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
     if (pre) {
       n0row = S.next * p.chunk_rows;
       nrows1 = min(p.chunk_rows, p.nrows - n0row);
-      for (uint32_t r = tid; r <= nrows1; r += kThreads) cp_async8(&S.u.a.arow[r], p.a_rowmap + uint64_t(n0row) + r);
+      if ((reinterpret_cast<uintptr_t>(p.a_rowmap) & 15u) == 0) {
+        // pairs of row pointers in 16-byte copies (chunks start at a multiple
+        // of 32 rows, so every pair is aligned in both spaces), the last odd one alone
+        for (uint32_t q = tid; q < (nrows1 + 1) / 2; q += kThreads)
+          cp_async16(&S.u.a.arow[2 * q], p.a_rowmap + uint64_t(n0row) + 2 * q);
+        if (tid == 0 && !(nrows1 & 1u)) cp_async8(&S.u.a.arow[nrows1], p.a_rowmap + uint64_t(n0row) + nrows1);
+      } else {
+        for (uint32_t r = tid; r <= nrows1; r += kThreads) cp_async8(&S.u.a.arow[r], p.a_rowmap + uint64_t(n0row) + r);
+      }
       cp_async_commit();
     }
     // the pending chunk: look-back, row map, one coalesced copy
