@@ -308,7 +308,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
       const uint32_t o = r ? incl[r - 1] : 0u;
       const uint32_t n = incl[r] - o;
       if (uint64_t(o) + n <= room) {
-        for (uint32_t k = 0; k < n; ++k) out[o + k] = S.slot[(spos + k) * kThreads + tid];
+        // a run (two entries at an even offset) a store
+        for (uint32_t k = 0; k < n; k += 2)
+          *reinterpret_cast<uint2*>(out + o + k) =
+              make_uint2(S.slot[(spos + k) * kThreads + tid], S.slot[(spos + k + 1) * kThreads + tid]);
       } else if (flag && n) {
         raise_flag(p, &p.ctl->overflow, 1ull);
       }
@@ -329,7 +332,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_spgemm_rowmode(FusedArgs p) {
                                            });
         if (c != n) raise_flag(p, &p.ctl->status, 8ull);
       } else {
-        for (uint32_t k = 0; k < n; ++k) out[o + k] = S.slot[(spos + k) * kThreads + tid];
+        for (uint32_t k = 0; k < n; k += 2)
+          *reinterpret_cast<uint2*>(out + o + k) =
+              make_uint2(S.slot[(spos + k) * kThreads + tid], S.slot[(spos + k + 1) * kThreads + tid]);
       }
       if (!(e & kGenLight)) spos += n;
     }
